@@ -1,0 +1,276 @@
+/*
+ * wlg.h — C-ABI of the B200 replica-exchange Wang–Landau (REWL) walker engine.
+ *
+ * The reference sampler (Faikert/replica_exchange_wang_landau, C++20) has no FFI layer;
+ * its drop-in seam is the C++ function
+ *
+ *     RewlResult run_rewl(const ParallelContext&, std::shared_ptr<const Couplings>,
+ *                         const RunConfig&);                 (include/wl/parallel.hpp:35-36)
+ *
+ * plus the physics helpers it is built from (include/wl/physics.hpp:37-84) and the
+ * per-walker API its tests drive (include/wl/wang_landau.hpp:91-175).  Every entry point
+ * below names the reference interface it replaces.  Conventions:
+ *   - every function returns a wlg_status (0 = ok); the message of the last failure on the
+ *     calling thread is returned by wlg_last_error();
+ *   - the engine owns all device memory; the caller owns every host buffer it passes;
+ *   - an engine is used from one host thread at a time;
+ *   - array arguments are plain host pointers with sizes; no torch or CUDA types appear.
+ */
+#ifndef WLG_H
+#define WLG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WLG_ABI_VERSION 1
+
+typedef enum wlg_status {
+    WLG_OK = 0,
+    WLG_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument in the reference            */
+    WLG_ERR_INIT_FAILED = 2,      /* walker initialisation failed (std::runtime_error)  */
+    WLG_ERR_ESCAPED = 3,          /* "Walker escaped its energy window"                 */
+    WLG_ERR_DEVICE = 4,           /* CUDA error, or no usable sm_100 device             */
+    WLG_ERR_TIMEOUT = 5,          /* a bounded device wait gave up                      */
+    WLG_ERR_RUNTIME = 6,          /* other std::runtime_error conditions                */
+    WLG_ERR_LOGIC = 7,            /* std::logic_error                                   */
+    WLG_ERR_OUT_OF_RANGE = 8,     /* std::out_of_range                                  */
+    WLG_ERR_IO = 9                /* file could not be read or written                  */
+} wlg_status;
+
+typedef enum wlg_precision {
+    WLG_PRECISION_FP64 = 0, /* J in FP64: bit-exact with the reference                  */
+    WLG_PRECISION_FP32 = 1, /* J in FP32, FP64 fields, periodic FP64 recompute          */
+    WLG_PRECISION_BF16 = 2  /* J in BF16 with a per-row FP32 scale, FP64 fields         */
+} wlg_precision;
+
+typedef enum wlg_stage { /* wl::RefinementStage (include/wl/wang_landau.hpp:58) */
+    WLG_STAGE_WANG_LANDAU = 0,
+    WLG_STAGE_INVERSE_TIME = 1,
+    WLG_STAGE_FROZEN = 2
+} wlg_stage;
+
+/* A dipolar Ising system: wl::Geometry + coupling scale + cutoff
+ * (include/wl/physics.hpp:13-35; apps/wl_run.cpp:81-83 selects CSR when cutoff > 0). */
+typedef struct wlg_system {
+    uint64_t n;               /* number of sites                                       */
+    const double* positions;  /* n x 3 (x, y, z), row-major                            */
+    const double* axes;       /* n x 3 unit easy axes                                  */
+    double box[3];            /* box lengths; a zero length leaves that axis open      */
+    int32_t periodic;         /* minimum image on the positive-length axes             */
+    double coupling_scale;    /* D                                                     */
+    double cutoff;            /* > 0 selects the CSR backend with |r| <= cutoff         */
+} wlg_system;
+
+/* wl::WlParameters (include/wl/wang_landau.hpp:40-56), field for field. */
+typedef struct wlg_wl_parameters {
+    double flatness;
+    uint64_t minimum_visits;
+    double final_factor;
+    uint64_t check_interval_attempts;
+    uint64_t force_accept_after_attempts;
+    int32_t inverse_time_enabled;
+    uint64_t initialization_max_attempts;
+    double initialization_target_fraction;
+    double initialization_temperature_fraction;
+    uint64_t initialization_stall_attempts_per_spin;
+    double initialization_temperature_multiplier;
+    double initialization_max_temperature_fraction;
+    int32_t collect_window_statistics;
+    double round_trip_margin_fraction;
+    int32_t nalivaiko_mod;
+} wlg_wl_parameters;
+
+/* The part of wl::RunConfig that run_rewl reads (include/wl/io.hpp:12-58), with MCS
+ * intervals already resolved to attempts (RunConfig::resolve_mcs, src/io.cpp:210-236). */
+typedef struct wlg_run_config {
+    double emin, emax, bin_width;           /* EnergyGrid                               */
+    uint64_t windows;                       /* energy windows                           */
+    uint64_t walkers_per_window;            /* RunConfig::walkers_per_rank              */
+    double overlap;                         /* partition_windows overlap                */
+    const uint64_t* explicit_windows;       /* NULL, or 2*windows (begin, end) bins     */
+    uint64_t seed;
+    wlg_wl_parameters wl;
+    uint64_t exchange_interval_attempts;
+    uint64_t max_attempts;                  /* 0 = run until every walker is frozen     */
+    uint64_t checkpoint_interval_attempts;
+    const char* checkpoint_path;            /* NULL/"" = none; used for 1 window x 1    */
+    const int8_t* initial_spins;            /* NULL, or windows*walkers x n spins       */
+    const uint8_t* initial_spins_present;   /* NULL = all present; else one per walker  */
+    double progress_interval_seconds;       /* 0 disables the progress line             */
+    int32_t coupling_precision;             /* wlg_precision                            */
+    uint64_t recompute_interval_attempts;   /* FP32/BF16 only: FP64 field recompute     */
+} wlg_run_config;
+
+/* wl::HistogramStatistics (include/wl/wang_landau.hpp:60-67). */
+typedef struct wlg_histogram_statistics {
+    uint64_t active_bins;
+    uint64_t covered_bins;
+    uint64_t minimum;
+    double mean;
+    double min_over_mean;
+    double coverage;
+} wlg_histogram_statistics;
+
+/* wl::WalkerStatistics (include/wl/io.hpp:60-75). */
+typedef struct wlg_walker_statistics {
+    uint64_t walker_id;
+    uint64_t window_id;
+    int32_t mpi_rank;
+    uint64_t attempted;
+    uint64_t accepted;
+    uint64_t forced_accepted;
+    uint64_t attempts_since_last_accepted;
+    double energy;
+    double factor;
+    uint64_t active_bins;
+    uint64_t minimum_histogram;
+    double mean_histogram;
+    double min_over_mean;
+    uint64_t round_trips;
+} wlg_walker_statistics;
+
+/* The scalar part of wl::RewlResult (include/wl/parallel.hpp:23-31). */
+typedef struct wlg_run_totals {
+    uint64_t attempted;
+    uint64_t accepted;
+    uint64_t forced_accepted;
+    uint64_t exchange_attempted;
+    uint64_t exchange_accepted;
+    int32_t converged;
+    uint64_t epochs;
+} wlg_run_totals;
+
+/* wl::WalkerSnapshot (include/wl/wang_landau.hpp:74-89).  The array members point to
+ * caller-owned buffers: spins and fields hold n entries, log_g/histogram/active hold
+ * grid-bins entries (the whole grid, as in the reference). */
+typedef struct wlg_snapshot {
+    uint64_t walker_id;
+    int8_t* spins;
+    double* fields;
+    double energy;
+    double* log_g;
+    uint64_t* histogram;
+    uint8_t* active;
+    double factor;
+    uint64_t attempted;
+    uint64_t accepted;
+    uint64_t forced_accepted;
+    uint64_t last_accepted_attempt;
+    uint8_t stage;
+    uint64_t rng_state[4];
+} wlg_snapshot;
+
+typedef struct wlg_engine wlg_engine;
+
+/* ---- library ------------------------------------------------------------------ */
+
+/* Returns WLG_ABI_VERSION. */
+int32_t wlg_abi_version(void);
+/* Message of the last failed call on this thread ("" if none). */
+const char* wlg_last_error(void);
+/* Fills defaults equal to the reference's RunConfig/WlParameters member initialisers
+ * (include/wl/io.hpp:12-58, include/wl/wang_landau.hpp:40-56) with MCS resolved for n
+ * spins as RunConfig::resolve_mcs does (src/io.cpp:210-236). */
+wlg_status wlg_default_run_config(uint64_t n, wlg_run_config* out);
+
+/* ---- host-side helpers (no GPU needed) ---------------------------------------- */
+
+/* EnergyGrid::bins / EnergyGrid::index (src/wang_landau.cpp:22-34).  *bin = -1 when the
+ * reference returns std::nullopt. */
+wlg_status wlg_grid_bins(double emin, double emax, double width, uint64_t* bins);
+wlg_status wlg_grid_index(double emin, double emax, double width, double energy, int64_t* bin);
+/* partition_windows (src/wang_landau.cpp:40-61); out holds 2*count (begin, end). */
+wlg_status wlg_partition_windows(uint64_t bins, uint64_t count, double overlap, uint64_t* out);
+/* Geometry::validate (src/physics.cpp:34-56). */
+wlg_status wlg_validate_system(const wlg_system* system);
+/* save_checkpoint / load_checkpoint: the WLCHKP3 binary format (src/io.cpp:539-572);
+ * load also reads WLCHKP1/WLCHKP2.  For load, sizes are returned first when the array
+ * pointers in *s are NULL (*n_spins, *n_bins set), then filled on a second call. */
+wlg_status wlg_checkpoint_save(const char* path, const wlg_snapshot* s, uint64_t n_spins,
+                               uint64_t n_bins);
+wlg_status wlg_checkpoint_load(const char* path, wlg_snapshot* s, uint64_t* n_spins,
+                               uint64_t* n_bins);
+
+/* ---- physics on the device ---------------------------------------------------- */
+
+/* DenseCouplings / CsrCouplings construction (src/physics.cpp:172-223), returned as the
+ * dense n x n matrix that Couplings::at(i, j) reads (zeros off the CSR pattern).  With
+ * precision FP32/BF16 the stored (rounded, row-scaled) values are returned as doubles. */
+wlg_status wlg_couplings_dense(const wlg_system* system, int32_t precision, double* out);
+/* CsrCouplings pattern (src/physics.cpp:197-223): row_offsets[n+1], columns[nnz],
+ * values[nnz].  Call with columns == NULL to get *nnz first. */
+wlg_status wlg_couplings_csr(const wlg_system* system, uint64_t* nnz, uint64_t* row_offsets,
+                             uint64_t* columns, double* values);
+/* local_fields + total_energy (src/physics.cpp:238-259) for `count` spin configurations
+ * (count x n spins), computed with the reference's summation order. */
+wlg_status wlg_local_fields(const wlg_system* system, const int8_t* spins, uint64_t count,
+                            double* fields, double* energies);
+
+/* ---- the REWL engine: run_rewl (src/parallel.cpp:276-747) ---------------------- */
+
+/* Builds J, constructs windows*walkers walkers (WangLandauWalker ctor with target
+ * Metropolis initialisation, src/wang_landau.cpp:63-242) and restores a checkpoint when
+ * the reference would (src/parallel.cpp:354-360). */
+wlg_status wlg_engine_create(const wlg_system* system, const wlg_run_config* config,
+                             wlg_engine** engine);
+void wlg_engine_destroy(wlg_engine* engine);
+/* The epoch loop of run_rewl (src/parallel.cpp:376-534) until every walker is frozen or
+ * the attempt limit is reached. */
+wlg_status wlg_engine_run(wlg_engine* engine, wlg_run_totals* totals);
+/* At most max_epochs epochs of the same loop; *done = 1 once the run has terminated. */
+wlg_status wlg_engine_run_epochs(wlg_engine* engine, uint64_t max_epochs,
+                                 uint64_t* epochs_run, int32_t* done);
+wlg_status wlg_engine_totals(wlg_engine* engine, wlg_run_totals* totals);
+uint64_t wlg_engine_walkers(const wlg_engine* engine);
+uint64_t wlg_engine_bins(const wlg_engine* engine);
+uint64_t wlg_engine_spins(const wlg_engine* engine);
+/* Window w as (begin, end) bins. */
+wlg_status wlg_engine_window(const wlg_engine* engine, uint64_t w, uint64_t* begin,
+                             uint64_t* end);
+/* summarize_walkers for window w (src/parallel.cpp:23-62, 170-179); arrays hold bins
+ * entries.  allow_empty mirrors allow_empty_intersection. */
+wlg_status wlg_engine_fragment(wlg_engine* engine, uint64_t w, int32_t allow_empty,
+                               double* log_g, uint64_t* histogram, double* standard_error,
+                               uint8_t* valid);
+/* summarize_sampling_impl (src/parallel.cpp:64-78). */
+wlg_status wlg_engine_sampling_statistics(wlg_engine* engine, uint64_t w,
+                                          double* squared_energy_displacement,
+                                          uint64_t* displacement_samples,
+                                          uint64_t* round_trips, uint64_t* walkers);
+/* RewlResult::walker_statistics (src/parallel.cpp:541-553); capacity >= walkers. */
+wlg_status wlg_engine_walker_statistics(wlg_engine* engine, wlg_walker_statistics* out,
+                                        uint64_t capacity);
+/* RewlResult::representatives (src/parallel.cpp:554-557): non-empty bank entries in
+ * walker order; energies[capacity], spins[capacity x n]. */
+wlg_status wlg_engine_representatives(wlg_engine* engine, double* energies, int8_t* spins,
+                                      uint64_t capacity, uint64_t* count);
+
+/* ---- single-walker operations (include/wl/wang_landau.hpp:98-138) -------------- */
+
+/* WangLandauWalker::run_attempts (src/wang_landau.cpp:286-288): count attempts on walker
+ * index `walker` only, without checks or exchange. */
+wlg_status wlg_walker_run_attempts(wlg_engine* engine, uint64_t walker, uint64_t count);
+/* snapshot / restore (src/wang_landau.cpp:415-466). */
+wlg_status wlg_walker_snapshot(wlg_engine* engine, uint64_t walker, wlg_snapshot* out);
+wlg_status wlg_walker_restore(wlg_engine* engine, uint64_t walker, const wlg_snapshot* in);
+/* histogram_statistics / flat / covered / ready_for_iteration / begin_next_iteration
+ * (src/wang_landau.cpp:344-409). */
+wlg_status wlg_walker_histogram_statistics(wlg_engine* engine, uint64_t walker,
+                                           wlg_histogram_statistics* out);
+wlg_status wlg_walker_flags(wlg_engine* engine, uint64_t walker, int32_t* flat,
+                            int32_t* covered, int32_t* ready);
+wlg_status wlg_walker_begin_next_iteration(wlg_engine* engine, uint64_t walker);
+/* exchange_log_probability / swap_configuration (src/wang_landau.cpp:483-508). */
+wlg_status wlg_walker_exchange_log_probability(wlg_engine* engine, uint64_t left,
+                                               uint64_t right, double* log_probability);
+wlg_status wlg_walker_swap(wlg_engine* engine, uint64_t left, uint64_t right);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WLG_H */

@@ -1,0 +1,209 @@
+// engine.hpp — host side of the REWL engine: device buffers, the Engine class that owns a
+// run (the replacement of run_rewl, src/parallel.cpp:276-747) and the kernel launchers.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/wlg.h"
+#include "common.cuh"
+
+namespace wlg {
+
+// An error carrying a wlg_status; the C-ABI layer turns it into a return code + message.
+struct WlgError : std::runtime_error {
+    wlg_status status;
+    WlgError(wlg_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+inline void check_cuda(cudaError_t e, const char* what) {
+    if (e != cudaSuccess)
+        throw WlgError(WLG_ERR_DEVICE, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
+}
+
+// Owning device allocation.
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    DeviceBuffer() = default;
+    explicit DeviceBuffer(size_t b) { allocate(b); }
+    DeviceBuffer(const DeviceBuffer&) = delete;
+    DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+    ~DeviceBuffer() { release(); }
+    void allocate(size_t b) {
+        release();
+        if (b == 0) b = 16;
+        check_cuda(cudaMalloc(&ptr, b), "cudaMalloc");
+        bytes = b;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <class T> T* get() const { return static_cast<T*>(ptr); }
+};
+
+// A system resident on the device: geometry plus the couplings built from it.
+struct DeviceSystem {
+    uint64_t n = 0;
+    uint64_t ld = 0;  // padded stride, multiple of 16
+    double box[3] = {0, 0, 0};
+    int32_t periodic = 0;
+    double scale = 1.0;
+    double cutoff = 0.0;
+    bool csr = false;
+    uint64_t nnz = 0;
+    DeviceBuffer pos, axes;
+    DeviceBuffer J64, J32, J16, Jscale;
+    DeviceBuffer csr_ptr, csr_col, csr_val64, csr_val32;
+};
+
+// Host-side validation and helpers (host.cpp).
+void validate_system(const wlg_system& s);
+void validate_grid(double emin, double emax, double width);
+uint64_t grid_bins(double emin, double emax, double width);
+std::vector<uint64_t> partition_windows(uint64_t bins, uint64_t count, double overlap);
+void upload_system(const wlg_system& s, DeviceSystem& d, cudaStream_t stream);
+void save_checkpoint_file(const std::string& path, const wlg_snapshot& s, uint64_t n, uint64_t bins);
+bool load_checkpoint_file(const std::string& path, std::vector<int8_t>& spins, std::vector<double>& fields,
+                          std::vector<double>& log_g, std::vector<uint64_t>& hist, std::vector<uint8_t>& active,
+                          wlg_snapshot& scalars, std::string& error);
+
+// physics.cu
+void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream);
+void compute_fields(const EngineView& v, const int8_t* spins, int64_t spin_stride, double* fields,
+                    int64_t field_stride, double* energies, int count, cudaStream_t stream);
+
+// Per-walker result of the target-Metropolis initialisation (the numbers the reference's
+// failure message prints, src/wang_landau.cpp:221-241).
+struct InitReport {
+    int32_t status;  // 0 ok, 1 did not reach the target band
+    int32_t pad;
+    double target;
+    double half_width;
+    double minimum_reached;
+    double maximum_reached;
+    double closest;
+    double closest_distance;
+    double highest_temperature;
+    uint64_t increases;
+    uint64_t restarts;
+    uint64_t stall;
+};
+
+struct WalkArgs {
+    int32_t first;          // first walker of the launch
+    int32_t count;          // walkers in the launch
+    uint64_t fixed_batch;   // > 0: exactly this many attempts, no check (run_attempts)
+    int32_t epoch_mode;     // 1: run_rewl batch + check + termination counters
+    int32_t smem_per_walker;
+};
+
+struct InitArgs {
+    int32_t smem_per_walker;
+    int32_t pad;
+    const int8_t* initial_spins;   // walkers x ld or null
+    const uint8_t* present;        // per walker
+    InitReport* reports;
+    uint64_t init_max_attempts;
+    double target_fraction;
+    double temperature_fraction;
+    uint64_t stall_per_spin;
+    double temperature_multiplier;
+    double max_temperature_fraction;
+};
+
+// walker.cu
+size_t walker_smem_bytes(const EngineView& v, bool smem_fields, bool features);
+bool fields_fit_in_smem(const EngineView& v, bool features);
+void launch_init(const EngineView& v, const InitArgs& a, int walkers_per_block, cudaStream_t stream);
+void launch_walk(const EngineView& v, const WalkArgs& a, int walkers_per_block, cudaStream_t stream);
+void launch_exchange(const EngineView& v, cudaStream_t stream);
+void launch_flush_pending(const EngineView& v, cudaStream_t stream);
+void launch_summarize(const EngineView& v, int window, int allow_empty, double* log_g, uint64_t* hist,
+                      double* sem, uint8_t* valid, int* status, cudaStream_t stream);
+void launch_sampling(const EngineView& v, int window, double* sq, uint64_t* samples, uint64_t* trips,
+                     cudaStream_t stream);
+void launch_walker_statistics(const EngineView& v, wlg_walker_statistics* out, cudaStream_t stream);
+void launch_histogram_statistics(const EngineView& v, int walker, wlg_histogram_statistics* out, int* flags,
+                                 cudaStream_t stream);
+void launch_begin_next_iteration(const EngineView& v, int walker, int* status, cudaStream_t stream);
+void launch_exchange_pair(const EngineView& v, int left, int right, int do_swap, double* logp, int* status,
+                          cudaStream_t stream);
+
+// The engine: one REWL run on the current device.
+class Engine {
+  public:
+    Engine(const wlg_system& system, const wlg_run_config& config);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    void run(wlg_run_totals* totals);
+    void run_epochs(uint64_t max_epochs, uint64_t* epochs_run, int32_t* done);
+    void totals(wlg_run_totals* out);
+    uint64_t walkers() const { return walkers_; }
+    uint64_t bins() const { return bins_; }
+    uint64_t spins() const { return sys_.n; }
+    void window(uint64_t w, uint64_t* begin, uint64_t* end) const;
+    void fragment(uint64_t w, int allow_empty, double* log_g, uint64_t* hist, double* sem, uint8_t* valid);
+    void sampling(uint64_t w, double* sq, uint64_t* samples, uint64_t* round_trips, uint64_t* walkers);
+    void walker_statistics(wlg_walker_statistics* out, uint64_t capacity);
+    void representatives(double* energies, int8_t* spins, uint64_t capacity, uint64_t* count);
+
+    void run_attempts(uint64_t walker, uint64_t count);
+    void snapshot(uint64_t walker, wlg_snapshot* out);
+    void restore(uint64_t walker, const wlg_snapshot& in);
+    void histogram_statistics(uint64_t walker, wlg_histogram_statistics* out, int32_t* flags);
+    void begin_next_iteration(uint64_t walker);
+    double exchange_log_probability(uint64_t left, uint64_t right);
+    void swap(uint64_t left, uint64_t right);
+
+    // Launch shape (chosen by the autotuner or set explicitly).
+    int walkers_per_block = 1;
+    int epochs_per_graph = 32;
+
+  private:
+    void initialise_walkers(const wlg_run_config& c);
+    void check_device_error();
+    void launch_epochs(uint64_t count);
+    void build_graph();
+    void maybe_checkpoint();
+    void print_progress(bool final_line);
+    std::vector<WalkerState> download_states();
+
+    wlg_run_config cfg_{};
+    DeviceParams p_{};
+    DeviceSystem sys_;
+    Grid grid_{};
+    uint64_t bins_ = 0, windows_ = 0, wpw_ = 0, walkers_ = 0;
+    std::vector<uint64_t> win_;  // 2 * windows
+    bool features_ = false;
+    bool smem_fields_ = true;
+    int precision_ = WLG_PRECISION_FP64;
+    cudaStream_t stream_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+    cudaGraph_t graph_ = nullptr;
+    int graph_epochs_ = 0;
+
+    DeviceBuffer d_win_begin_, d_win_end_, d_ws_, d_log_g_, d_hist_, d_active_, d_refine_, d_sqdisp_,
+        d_dsamples_, d_spins_, d_fields_, d_rep_energy_, d_rep_dist_, d_rep_target_, d_rep_present_,
+        d_rep_spins_, d_ctl_, d_scratch_;
+    EngineView view_{};
+
+    std::string checkpoint_path_;
+    bool checkpointing_ = false;
+    uint64_t last_checkpoint_ = 0;
+    bool done_ = false;
+    uint64_t epochs_ = 0;
+    double next_progress_ = 0.0;
+    size_t progress_width_ = 0;
+};
+
+}  // namespace wlg

@@ -1,0 +1,268 @@
+// physics.cu — coupling construction and local fields on the device.
+//
+//  * dense_build_kernel: DenseCouplings (src/physics.cpp:172-184).  One 32x32 tile of
+//    pairs (i < j) per CTA; each pair is evaluated once, in the reference's orientation
+//    (displacement r_j - r_i, axes e_i then e_j), and written to both triangles through a
+//    shared-memory transpose so both stores are coalesced.
+//  * csr_count_kernel / csr_fill_kernel: CsrCouplings (src/physics.cpp:197-223).  One warp
+//    per row; columns are visited in increasing order and compacted with a ballot, which
+//    yields the reference's (row, column) sort order without sorting.
+//  * fields_kernel / energy_kernel: local_fields and total_energy (src/physics.cpp:
+//    238-259) with the reference's sequential summation order.
+//
+// All three are set-up kernels (O(N^2) once per system); the sampling hot path is in
+// walker.cu.
+#include "engine.hpp"
+
+namespace wlg {
+
+struct SystemView {
+    const double* pos;   // n x 3
+    const double* axes;  // n x 3
+    double box[3];
+    int32_t periodic;
+    double scale;
+    double cutoff;
+    int32_t n;
+};
+
+// minimum_image (src/physics.cpp:151-160)
+__device__ __forceinline__ void minimum_image(const SystemView& s, double& dx, double& dy, double& dz) {
+    if (!s.periodic) return;
+    if (s.box[0] > 0.0) dx -= s.box[0] * rint(dx / s.box[0]);
+    if (s.box[1] > 0.0) dy -= s.box[1] * rint(dy / s.box[1]);
+    if (s.box[2] > 0.0) dz -= s.box[2] * rint(dz / s.box[2]);
+}
+
+// pair_for + dipolar_pair (src/physics.cpp:26-30, 162-170) for a < b.  Returns false for
+// coincident sites.  `dist` receives norm(d) for the CSR cutoff test.
+__device__ __forceinline__ bool pair_value(const SystemView& s, int a, int b, double& value, double& dist) {
+    double dx = s.pos[3 * b] - s.pos[3 * a];
+    double dy = s.pos[3 * b + 1] - s.pos[3 * a + 1];
+    double dz = s.pos[3 * b + 2] - s.pos[3 * a + 2];
+    minimum_image(s, dx, dy, dz);
+    const double r2 = dx * dx + dy * dy + dz * dz;
+    dist = sqrt(r2);
+    if (!(r2 > 0.0)) { value = 0.0; return false; }
+    const double inv_r = 1.0 / sqrt(r2);
+    const double rx = dx * inv_r, ry = dy * inv_r, rz = dz * inv_r;
+    const double* ai = s.axes + 3 * a;
+    const double* aj = s.axes + 3 * b;
+    const double dot_ij = ai[0] * aj[0] + ai[1] * aj[1] + ai[2] * aj[2];
+    const double dot_ir = ai[0] * rx + ai[1] * ry + ai[2] * rz;
+    const double dot_jr = aj[0] * rx + aj[1] * ry + aj[2] * rz;
+    const double angular = dot_ij - 3.0 * dot_ir * dot_jr;
+    value = s.scale * angular * inv_r * inv_r * inv_r;
+    return true;
+}
+
+__global__ void dense_build_kernel(SystemView s, int ld, double* __restrict__ J, int* __restrict__ err) {
+    const int bi = blockIdx.y, bj = blockIdx.x;
+    if (bi > bj) return;
+    __shared__ double tile[32][33];
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = bi * 32 + r, j = bj * 32 + threadIdx.x;
+        double v = 0.0;
+        if (i < s.n && j < s.n && i < j) {
+            double dist;
+            if (!pair_value(s, i, j, v, dist)) atomicExch(err, 1);
+        }
+        tile[r][threadIdx.x] = v;
+        if (i < ld && j < ld && i <= j) J[static_cast<size_t>(i) * ld + j] = v;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int j = bj * 32 + r, i = bi * 32 + threadIdx.x;
+        if (i < ld && j < ld && i < j) J[static_cast<size_t>(j) * ld + i] = tile[threadIdx.x][r];
+    }
+}
+
+// One warp per row: count the columns c != row with norm(d) <= cutoff.
+__global__ void csr_count_kernel(SystemView s, int32_t* __restrict__ counts, int* __restrict__ err) {
+    const int lane = threadIdx.x & 31;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (row >= s.n) return;
+    int total = 0;
+    for (int c0 = 0; c0 < s.n; c0 += 32) {
+        const int c = c0 + lane;
+        bool in = false;
+        if (c < s.n && c != row) {
+            double v, dist;
+            const bool ok = pair_value(s, min(row, c), max(row, c), v, dist);
+            in = dist <= s.cutoff;
+            if (in && !ok) atomicExch(err, 1);
+        }
+        total += __popc(__ballot_sync(0xffffffffu, in));
+    }
+    if (lane == 0) counts[row] = total;
+}
+
+__global__ void csr_fill_kernel(SystemView s, const int32_t* __restrict__ ptr, int32_t* __restrict__ col,
+                                double* __restrict__ val64, float* __restrict__ val32) {
+    const int lane = threadIdx.x & 31;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (row >= s.n) return;
+    int base = ptr[row];
+    for (int c0 = 0; c0 < s.n; c0 += 32) {
+        const int c = c0 + lane;
+        bool in = false;
+        double v = 0.0;
+        if (c < s.n && c != row) {
+            double dist;
+            pair_value(s, min(row, c), max(row, c), v, dist);
+            in = dist <= s.cutoff;
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, in);
+        if (in) {
+            const int at = base + __popc(mask & ((1u << lane) - 1u));
+            col[at] = c;
+            val64[at] = v;
+            if (val32) val32[at] = static_cast<float>(v);
+        }
+        base += __popc(mask);
+    }
+}
+
+// Row-scaled BF16 copy: scale_i = max_j |J_ij| (as float), q_ij = bf16(J_ij / scale_i).
+__global__ void dense_lowp_kernel(const double* __restrict__ J, int n, int ld, float* __restrict__ J32,
+                                  __nv_bfloat16* __restrict__ J16, float* __restrict__ scale) {
+    const int row = blockIdx.x;
+    __shared__ double red[32];
+    double mx = 0.0;
+    for (int j = threadIdx.x; j < ld; j += blockDim.x) mx = fmax(mx, fabs(J[static_cast<size_t>(row) * ld + j]));
+    for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        mx = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        for (int o = 16; o; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (threadIdx.x == 0) red[0] = mx;
+    }
+    __syncthreads();
+    const float sc = red[0] > 0.0 ? static_cast<float>(red[0]) : 1.0f;
+    if (threadIdx.x == 0 && scale) scale[row] = sc;
+    for (int j = threadIdx.x; j < ld; j += blockDim.x) {
+        const double x = J[static_cast<size_t>(row) * ld + j];
+        if (J32) J32[static_cast<size_t>(row) * ld + j] = static_cast<float>(x);
+        if (J16) J16[static_cast<size_t>(row) * ld + j] = __double2bfloat16(x / static_cast<double>(sc));
+    }
+    (void)n;
+}
+
+// local_fields for `count` configurations: thread per (config, site), sequential in j.
+__global__ void fields_kernel(EngineView v, const int8_t* __restrict__ spins, int64_t spin_stride,
+                              double* __restrict__ fields, int64_t field_stride, int count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (i >= v.n || k >= count) return;
+    const int8_t* s = spins + k * spin_stride;
+    double sum = 0.0;
+    if (!v.csr) {
+        for (int j = 0; j < v.n; ++j) sum += v.J64[static_cast<size_t>(j) * v.ld + i] * static_cast<double>(s[j]);
+    } else {
+        for (int q = v.csr_ptr[i]; q < v.csr_ptr[i + 1]; ++q)
+            sum += v.csr_val64[q] * static_cast<double>(s[v.csr_col[q]]);
+    }
+    fields[k * field_stride + i] = sum;
+}
+
+// total_energy: one thread per configuration, sequential over i.
+__global__ void energy_kernel(int n, const int8_t* __restrict__ spins, int64_t spin_stride,
+                              const double* __restrict__ fields, int64_t field_stride, double* __restrict__ out,
+                              int count) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    double e = 0.0;
+    for (int i = 0; i < n; ++i)
+        e += 0.5 * static_cast<double>(spins[k * spin_stride + i]) * fields[k * field_stride + i];
+    out[k] = e;
+}
+
+// ---- host launchers ------------------------------------------------------------------
+
+static SystemView make_view(const DeviceSystem& d) {
+    SystemView s;
+    s.pos = d.pos.get<double>();
+    s.axes = d.axes.get<double>();
+    for (int k = 0; k < 3; ++k) s.box[k] = d.box[k];
+    s.periodic = d.periodic;
+    s.scale = d.scale;
+    s.cutoff = d.cutoff;
+    s.n = static_cast<int32_t>(d.n);
+    return s;
+}
+
+void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream) {
+    const SystemView s = make_view(d);
+    DeviceBuffer err(sizeof(int));
+    check_cuda(cudaMemsetAsync(err.ptr, 0, sizeof(int), stream), "memset");
+    const int n = static_cast<int>(d.n);
+    if (!d.csr) {
+        d.J64.allocate(d.ld * d.ld * sizeof(double));
+        check_cuda(cudaMemsetAsync(d.J64.ptr, 0, d.J64.bytes, stream), "memset J");
+        const int tiles = static_cast<int>((d.ld + 31) / 32);
+        dense_build_kernel<<<dim3(tiles, tiles), dim3(32, 8), 0, stream>>>(s, static_cast<int>(d.ld),
+                                                                           d.J64.get<double>(), err.get<int>());
+        check_cuda(cudaGetLastError(), "dense_build_kernel");
+        if (precision == WLG_PRECISION_FP32) d.J32.allocate(d.ld * d.ld * sizeof(float));
+        if (precision == WLG_PRECISION_BF16) {
+            d.J16.allocate(d.ld * d.ld * sizeof(__nv_bfloat16));
+            d.Jscale.allocate(d.ld * sizeof(float));
+        }
+        if (precision != WLG_PRECISION_FP64) {
+            dense_lowp_kernel<<<static_cast<unsigned>(d.ld), 256, 0, stream>>>(
+                d.J64.get<double>(), n, static_cast<int>(d.ld), d.J32.get<float>(), d.J16.get<__nv_bfloat16>(),
+                d.Jscale.get<float>());
+            check_cuda(cudaGetLastError(), "dense_lowp_kernel");
+        }
+    } else {
+        DeviceBuffer counts(static_cast<size_t>(n) * sizeof(int32_t));
+        const int warps_per_block = 8;
+        const unsigned blocks = static_cast<unsigned>((n + warps_per_block - 1) / warps_per_block);
+        csr_count_kernel<<<blocks, 32 * warps_per_block, 0, stream>>>(s, counts.get<int32_t>(), err.get<int>());
+        check_cuda(cudaGetLastError(), "csr_count_kernel");
+        std::vector<int32_t> host_counts(static_cast<size_t>(n));
+        check_cuda(cudaMemcpyAsync(host_counts.data(), counts.ptr, counts.bytes, cudaMemcpyDeviceToHost, stream),
+                   "copy counts");
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        std::vector<int32_t> ptr(static_cast<size_t>(n) + 1, 0);
+        int64_t total = 0;
+        for (int i = 0; i < n; ++i) {
+            total += host_counts[static_cast<size_t>(i)];
+            if (total > INT32_MAX) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "CSR has more than 2^31 couplings");
+            ptr[static_cast<size_t>(i) + 1] = static_cast<int32_t>(total);
+        }
+        d.nnz = static_cast<uint64_t>(total);
+        d.csr_ptr.allocate(ptr.size() * sizeof(int32_t));
+        check_cuda(cudaMemcpyAsync(d.csr_ptr.ptr, ptr.data(), d.csr_ptr.bytes, cudaMemcpyHostToDevice, stream),
+                   "copy ptr");
+        const size_t nnz = std::max<size_t>(1, static_cast<size_t>(total));
+        d.csr_col.allocate(nnz * sizeof(int32_t));
+        d.csr_val64.allocate(nnz * sizeof(double));
+        if (precision == WLG_PRECISION_FP32) d.csr_val32.allocate(nnz * sizeof(float));
+        csr_fill_kernel<<<blocks, 32 * warps_per_block, 0, stream>>>(s, d.csr_ptr.get<int32_t>(),
+                                                                     d.csr_col.get<int32_t>(),
+                                                                     d.csr_val64.get<double>(),
+                                                                     d.csr_val32.get<float>());
+        check_cuda(cudaGetLastError(), "csr_fill_kernel");
+    }
+    int host_err = 0;
+    check_cuda(cudaMemcpyAsync(&host_err, err.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream), "copy err");
+    check_cuda(cudaStreamSynchronize(stream), "sync");
+    if (host_err) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Coincident dipole sites");
+}
+
+void compute_fields(const EngineView& v, const int8_t* spins, int64_t spin_stride, double* fields,
+                    int64_t field_stride, double* energies, int count, cudaStream_t stream) {
+    if (count <= 0) return;
+    const dim3 grid(static_cast<unsigned>((v.n + 127) / 128), static_cast<unsigned>(count));
+    fields_kernel<<<grid, 128, 0, stream>>>(v, spins, spin_stride, fields, field_stride, count);
+    check_cuda(cudaGetLastError(), "fields_kernel");
+    if (energies) {
+        energy_kernel<<<static_cast<unsigned>((count + 127) / 128), 128, 0, stream>>>(
+            v.n, spins, spin_stride, fields, field_stride, energies, count);
+        check_cuda(cudaGetLastError(), "energy_kernel");
+    }
+}
+
+}  // namespace wlg

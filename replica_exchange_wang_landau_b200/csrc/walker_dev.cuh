@@ -1,0 +1,153 @@
+// walker_dev.cuh — warp-level pieces of WangLandauWalker used by several kernels.
+//
+// A walker is owned by one warp.  All 32 lanes evaluate the walker's scalar chain
+// redundantly (identical registers, no divergence, no shuffles on the hot path); the
+// lanes split only the O(N) / O(z) field updates and the O(bins) histogram reductions.
+// Shared-memory writes of scalars are done by lane 0 and published with __syncwarp().
+#pragma once
+
+#include "common.cuh"
+
+namespace wlg {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint64_t warp_sum_u64(uint64_t x) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+    return x;
+}
+
+__device__ __forceinline__ uint64_t warp_min_u64(uint64_t x) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        const uint64_t y = __shfl_xor_sync(kFull, x, o);
+        x = y < x ? y : x;
+    }
+    return x;
+}
+
+// histogram_statistics (src/wang_landau.cpp:344-367) over the window slice [0, nbins) of
+// h / mask.  active_bins is the walker's cached counter, as in the reference.
+struct HistStats {
+    uint64_t active_bins;
+    uint64_t covered;
+    uint64_t minimum;
+    double mean;
+    double min_over_mean;
+    double coverage;
+};
+
+__device__ __forceinline__ HistStats warp_histogram_statistics(const uint64_t* h, const uint8_t* mask, int nbins,
+                                                               uint64_t active_bins, int lane) {
+    uint64_t covered = 0, mn = ~0ULL, total = 0;
+    for (int b = lane; b < nbins; b += 32) {
+        if (!mask[b]) continue;
+        const uint64_t v = h[b];
+        covered += v != 0 ? 1 : 0;
+        mn = v < mn ? v : mn;
+        total += v;
+    }
+    covered = warp_sum_u64(covered);
+    mn = warp_min_u64(mn);
+    total = warp_sum_u64(total);
+    HistStats s;
+    s.active_bins = active_bins;
+    s.covered = covered;
+    s.minimum = mn;
+    s.mean = 0.0;
+    s.min_over_mean = 0.0;
+    s.coverage = 0.0;
+    if (active_bins == 0) {
+        s.minimum = 0;
+        return s;
+    }
+    s.mean = x87_mean(total, active_bins);
+    s.min_over_mean = s.mean > 0.0 ? static_cast<double>(s.minimum) / s.mean : 0.0;
+    s.coverage = static_cast<double>(covered) / static_cast<double>(active_bins);
+    return s;
+}
+
+// flat / covered / ready_for_iteration (src/wang_landau.cpp:369-387)
+__device__ __forceinline__ bool stats_flat(const HistStats& s, int32_t stage, const DeviceParams& p) {
+    if (stage != kWangLandau) return true;
+    return s.active_bins != 0 && s.minimum >= p.minimum_visits && s.min_over_mean >= p.flatness;
+}
+__device__ __forceinline__ bool stats_covered(const HistStats& s, int32_t stage) {
+    if (stage != kWangLandau) return true;
+    return s.active_bins != 0 && s.covered == s.active_bins;
+}
+__device__ __forceinline__ bool stats_ready(const HistStats& s, int32_t stage, const DeviceParams& p) {
+    return stage == kWangLandau && (p.inverse_time ? stats_covered(s, stage) : stats_flat(s, stage, p));
+}
+
+// begin_next_iteration + freeze_if_finished (src/wang_landau.cpp:389-413); the caller has
+// checked readiness.  h / refine are the window slices.
+__device__ __forceinline__ void warp_begin_next_iteration(WalkerState& st, uint64_t* h, uint8_t* refine, int nbins,
+                                                          const DeviceParams& p, int lane) {
+    st.factor *= 0.5;
+    for (int b = lane; b < nbins; b += 32) h[b] = 0;
+    if (p.nalivaiko) {
+        for (int b = lane; b < nbins; b += 32) refine[b] = 0;
+        st.refine_count = 0;
+    }
+    if (p.inverse_time) {
+        const double inverse_time = st.attempted == 0
+                                        ? 1.0
+                                        : static_cast<double>(st.active_count) / static_cast<double>(st.attempted);
+        if (st.factor <= inverse_time) {
+            st.stage = kInverseTime;
+            st.factor = inverse_time;
+        }
+    }
+    if (st.factor <= p.final_factor) st.stage = kFrozen;
+    __syncwarp();
+}
+
+// update_round_trip_state (src/wang_landau.cpp:317-330)
+__device__ __forceinline__ void round_trip_update(double energy, double lower, double upper, double margin_fraction,
+                                                  int32_t& state, uint64_t& trips) {
+    const double margin = margin_fraction * (upper - lower);
+    if (energy <= lower + margin) {
+        if (state == 2) {
+            ++trips;
+            state = 1;
+        } else if (state == 0) {
+            state = 1;
+        }
+    } else if (energy >= upper - margin && state == 1) {
+        state = 2;
+    }
+}
+
+// update_representatives (src/wang_landau.cpp:332-342); spins is the walker's current
+// configuration (shared or global memory), n bytes, copied by the whole warp.
+__device__ __forceinline__ void warp_update_representatives(const EngineView& v, int walker, double energy,
+                                                            const int8_t* spins, int lane) {
+    for (int r = 0; r < kRepresentatives; ++r) {
+        const size_t q = static_cast<size_t>(walker) * kRepresentatives + r;
+        const double distance = fabs(energy - v.rep_target[q]);
+        if (distance < v.rep_dist[q]) {
+            int8_t* dst = v.rep_spins + q * static_cast<size_t>(v.ld);
+            for (int i = lane; i < v.ld; i += 32) dst[i] = spins[i];
+            __syncwarp();
+            if (lane == 0) {
+                v.rep_dist[q] = distance;
+                v.rep_energy[q] = energy;
+                v.rep_present[q] = 1;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+__device__ __forceinline__ double window_lower(const EngineView& v, int wb) {
+    return v.grid.minimum + static_cast<double>(wb) * v.grid.width;
+}
+
+__device__ __forceinline__ void record_error(Control* ctl, int status, int walker) {
+    if (atomicCAS(&ctl->error, 0, status) == 0) ctl->error_walker = walker;
+    ctl->done = 1;
+}
+
+}  // namespace wlg
