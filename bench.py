@@ -1,0 +1,356 @@
+"""Benchmark: spin-flip attempts/s of the dense REWL workload on B200.
+
+Workload (the configuration the reference's headline metric is quoted on): an 8x8x8 simple
+cubic lattice (N = 512), periodic box 8, D = 1, easy axes uniform on the unit sphere
+(random_sphere_axes, seed 1), dense FP64 minimum-image couplings; 16 energy windows at 75%
+overlap x 8 walkers = 128 walkers; replica exchange every 1 MCS (512 attempts); bins of 0.5
+over the pilot range +5% ([-228.5, 228.0], 913 bins; pilot: the reference's `wl_run --pilot`
+infinite-temperature walk of 1e5 MCS on this system, seed 1).  Synthetic data: the system
+is generated from its seed; no dataset is involved.
+
+A step is `--epochs-per-step` epochs; an epoch is one exchange interval of attempts for
+every walker, the walker-local check and one even/odd exchange (run_rewl's loop body).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank runs an independent replica of the workload (the north
+star fixes one GPU per run; windows are not sharded), timed on the device, max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "spin-flip attempts/s"
+UNIT = "attempts/s"
+WORKLOAD = ("dense REWL: 8x8x8 simple cubic N=512, periodic box 8, random-sphere axes (seed 1), dense FP64 J; "
+            "16 windows x 8 walkers at 75% overlap; exchange every 1 MCS; bin 0.5 on [-228.5, 228.0]")
+EMIN, EMAX, WIDTH = -228.5, 228.0, 0.5
+
+
+def make_workload(seed: int):
+    from replica_exchange_wang_landau_b200.engine import RunConfig, System
+    from replica_exchange_wang_landau_b200.geometry import simple_cubic_random
+    geometry = simple_cubic_random(8, 8, 8, seed=1, periodic=True)
+    system = System(geometry, 1.0, 0.0)
+    config = RunConfig(emin=EMIN, emax=EMAX, bin_width=WIDTH, windows=16, walkers=8, overlap=0.75, seed=seed,
+                       exchange_interval_mcs=1.0)
+    config.resolve_mcs(geometry.size())
+    return system, config
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def ncu_traffic_per_launch():
+    """dram bytes per sweep-kernel launch from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "walk_kernel_dense_rewl_n512.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.file.flush()
+        rows = []
+        try:
+            for line in Path(self.file.name).read_text().splitlines():
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            os.unlink(self.file.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def flush_l2(torch, buf):
+    buf.add_(1.0)  # 256 MiB written: larger than the 126 MB L2
+
+
+def run_ours(args, rank: int, world: int, dist, torch) -> None:
+    from replica_exchange_wang_landau_b200 import engine as E
+    from replica_exchange_wang_landau_b200._abi import wlg_run_config
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    E.set_device(local)
+    torch.cuda.set_device(local)
+    system, config = make_workload(seed=1 + rank)
+    n = system.size()
+    flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    eng = E.Engine(system, config)
+    epochs = args.epochs_per_step
+    for _ in range(args.warmup):
+        eng.time_epochs(epochs)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    walk_ms = exch_ms = total_ms = 0.0
+    attempted = accepted = 0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush_l2(torch, flush)
+            torch.cuda.synchronize()
+            t = eng.time_epochs(epochs)
+            walk_ms += t["walk_ms"]
+            exch_ms += t["exchange_ms"]
+            total_ms += t["total_ms"]
+            attempted += t["attempted"]
+            accepted += t["accepted"]
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clock = clocks.summary()
+    # max over ranks of the device time; total attempts over ranks
+    if dist:
+        tt = torch.tensor([total_ms, walk_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        at = torch.tensor([attempted, accepted], dtype=torch.float64, device="cuda")
+        dist.all_reduce(at, op=dist.ReduceOp.SUM)
+        total_max, walk_max = float(tt[0]), float(tt[1])
+        att_all, acc_all = int(at[0]), int(at[1])
+    else:
+        total_max, walk_max, att_all, acc_all = total_ms, walk_ms, attempted, accepted
+    value = att_all / (total_max / 1e3)
+
+    # graph-replay throughput of the product path (run_epochs), same workload, for context
+    torch.cuda.synchronize()
+    g0 = time.perf_counter()
+    before = eng.totals()["attempted"]
+    eng.run_epochs(epochs * min(args.steps, 5))
+    torch.cuda.synchronize()
+    graph_rate = (eng.totals()["attempted"] - before) / (time.perf_counter() - g0)
+    eng.close()
+
+    # e2e through the C-ABI with pinned host buffers: create (H2D geometry) -> run -> fragments (D2H)
+    lib = E.load_library()
+    pos = torch.from_numpy(system.geometry.positions.copy()).pin_memory()
+    axes = torch.from_numpy(system.geometry.axes.copy()).pin_memory()
+    from replica_exchange_wang_landau_b200.engine import Geometry, System
+    pinned_system = System(Geometry(pos.numpy(), axes.numpy(), system.geometry.box, True), 1.0, 0.0)
+    bins = config.bins()
+    out_lg = torch.empty(bins, dtype=torch.float64).pin_memory()
+    out_h = torch.empty(bins, dtype=torch.int64).pin_memory()
+    out_se = torch.empty(bins, dtype=torch.float64).pin_memory()
+    out_v = torch.empty(bins, dtype=torch.uint8).pin_memory()
+    p_lg = C.cast(out_lg.data_ptr(), C.POINTER(C.c_double))
+    p_h = C.cast(out_h.data_ptr(), C.POINTER(C.c_uint64))
+    p_se = C.cast(out_se.data_ptr(), C.POINTER(C.c_double))
+    p_v = C.cast(out_v.data_ptr(), C.POINTER(C.c_uint8))
+    e2e_steps = max(1, min(args.steps, 5))
+    e2e_time = 0.0
+    e2e_attempts = 0
+    h2d = 2 * n * 3 * 8
+    d2h = config.windows * bins * (8 + 8 + 8 + 1)
+    for k in range(e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sys_s = pinned_system._struct()
+        cfg_s, keep = config._struct(n)
+        handle = C.c_void_p()
+        E._check(lib.wlg_engine_create(C.byref(sys_s), C.byref(cfg_s), C.byref(handle)))
+        ran, done = C.c_uint64(0), C.c_int32(0)
+        E._check(lib.wlg_engine_run_epochs(handle, epochs, C.byref(ran), C.byref(done)))
+        for w in range(config.windows):
+            E._check(lib.wlg_engine_fragment(handle, w, 0, p_lg, p_h, p_se, p_v))
+        totals = E._abi.wlg_run_totals()
+        E._check(lib.wlg_engine_totals(handle, C.byref(totals)))
+        lib.wlg_engine_destroy(handle)
+        dt = time.perf_counter() - t0
+        if k > 0:  # the first call is a warm-up (module load, kernel attributes)
+            e2e_time += dt
+            e2e_attempts += totals.attempted
+    e2e_value = e2e_attempts / e2e_time
+    if dist:
+        et = torch.tensor([e2e_time], dtype=torch.float64, device="cuda")
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+        ea = torch.tensor([e2e_attempts], dtype=torch.float64, device="cuda")
+        dist.all_reduce(ea, op=dist.ReduceOp.SUM)
+        e2e_value = float(ea[0]) / float(et[0])
+
+    # roofline of the sweep kernel: algorithmic bytes = one FP64 J row (N x 8 bytes) per
+    # accepted flip (fields, spins and the window's log_g/H live in shared memory)
+    peaks = load_peaks()
+    launches = args.steps * epochs
+    bytes_per_launch = accepted * n * 8 / launches
+    launch_s = (walk_ms / launches) / 1e3
+    achieved = bytes_per_launch / launch_s / 1e9
+    traffic = ncu_traffic_per_launch()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_sample_mcs)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD, "walkers": 128, "spins": n, "epochs_per_step": epochs,
+                       "attempts_per_step_per_gpu": attempted // args.steps,
+                       "l2": "flushed between timed steps (256 MiB write); J (2 MB) is L2-resident within a step",
+                       "parallelism": f"{world} independent replica(s), one per GPU"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "steps": e2e_steps, "path": "wlg_engine_create -> wlg_engine_run_epochs -> wlg_engine_fragment "
+                                                "x16 -> wlg_engine_destroy, pinned host buffers"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                         "kernel": "walk_kernel<FP64,dense>", "peak_source": peaks["source"],
+                         "bytes_per_launch": bytes_per_launch, "launch_ms": launch_s * 1e3,
+                         "acceptance": accepted / max(1, attempted)},
+            "gpu_launches": 2 * launches,
+            "graph_replay_attempts_per_s": graph_rate,
+            "clocks": clock,
+            "exchange_ms_per_step": exch_ms / args.steps,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line))
+
+
+def reference_rate(mcs: float, threads: int, seed: int = 1):
+    from oracle.oracle import Reference
+    ref = Reference()
+    used = ref.set_threads(threads)
+    system, config = make_workload(seed=seed)
+    config.max_mcs = mcs
+    config.resolved_spin_count = 0
+    config.resolve_mcs(system.size())
+    t0 = time.perf_counter()
+    r = ref.run_rewl(system, config)
+    dt = time.perf_counter() - t0
+    return r.attempted, dt, used
+
+
+def cpu_baseline(sample_mcs: float) -> dict:
+    threads = os.cpu_count() or 1
+    attempted, dt, used = reference_rate(sample_mcs, threads)
+    return {"value": attempted / dt, "unit": UNIT, "cores": used, "kind": "reference",
+            "sample": f"reference run_rewl (oracle/_ref, built from the reference sources, OpenMP) on the same "
+                      f"system and 16x8 walkers, {sample_mcs:g} MCS per walker including walker construction, "
+                      f"{dt:.2f} s"}
+
+
+def run_reference(args, rank: int) -> None:
+    if rank != 0:
+        return
+    from oracle.oracle import reference_available
+    if not reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libwlref.so was not built"}))
+        return
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        reference_rate(args.reference_step_mcs, threads)
+    total_t = 0.0
+    total_a = 0
+    used = threads
+    for _ in range(args.steps):
+        a, dt, used = reference_rate(args.reference_step_mcs, threads)
+        total_t += dt
+        total_a += a
+    value = total_a / total_t
+    sample = (f"reference run_rewl per step (oracle/_ref, compiled from the reference sources, OpenMP over walkers) "
+              f"on the same system and 16x8 walkers, {args.reference_step_mcs:g} MCS per walker per step, walker "
+              f"construction included")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total_t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+        "config": {"workload": WORKLOAD, "walkers": 128, "spins": 512},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--epochs-per-step", type=int, default=100)
+    ap.add_argument("--cpu-sample-mcs", type=float, default=400.0)
+    ap.add_argument("--reference-step-mcs", type=float, default=50.0)
+    ap.add_argument("--skip-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as td
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = td
+    try:
+        run_ours(args, rank, world, dist, torch)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

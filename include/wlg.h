@@ -144,6 +144,17 @@ typedef struct wlg_run_totals {
     uint64_t epochs;
 } wlg_run_totals;
 
+/* Device timing of a run of epochs (no counterpart in the reference, which only reports
+ * wall-clock time, apps/wl_run.cpp:175-178). */
+typedef struct wlg_epoch_timing {
+    uint64_t epochs;     /* epochs run                                                   */
+    double walk_ms;      /* device time of the sweep kernels (CUDA events)               */
+    double exchange_ms;  /* device time of the exchange kernels                          */
+    double total_ms;     /* device time from the first launch to the last                */
+    uint64_t attempted;  /* attempts made in these epochs, all walkers                   */
+    uint64_t accepted;   /* accepted flips in these epochs, all walkers                  */
+} wlg_epoch_timing;
+
 /* wl::WalkerSnapshot (include/wl/wang_landau.hpp:74-89).  The array members point to
  * caller-owned buffers: spins and fields hold n entries, log_g/histogram/active hold
  * grid-bins entries (the whole grid, as in the reference). */
@@ -172,6 +183,10 @@ typedef struct wlg_engine wlg_engine;
 int32_t wlg_abi_version(void);
 /* Message of the last failed call on this thread ("" if none). */
 const char* wlg_last_error(void);
+/* Selects the CUDA device that engines created afterwards on this thread use (the
+ * library carries its own CUDA runtime).  One process per GPU is the intended layout.  No
+ * counterpart in the reference, which is CPU-only. */
+wlg_status wlg_set_device(int32_t device);
 /* Fills defaults equal to the reference's RunConfig/WlParameters member initialisers
  * (include/wl/io.hpp:12-58, include/wl/wang_landau.hpp:40-56) with MCS resolved for n
  * spins as RunConfig::resolve_mcs does (src/io.cpp:210-236). */
@@ -225,6 +240,13 @@ wlg_status wlg_engine_run(wlg_engine* engine, wlg_run_totals* totals);
 wlg_status wlg_engine_run_epochs(wlg_engine* engine, uint64_t max_epochs,
                                  uint64_t* epochs_run, int32_t* done);
 wlg_status wlg_engine_totals(wlg_engine* engine, wlg_run_totals* totals);
+/* The same epochs as wlg_engine_run_epochs, launched one kernel at a time with CUDA events
+ * around each kernel on the engine's stream (profiling; no counterpart in the reference). */
+wlg_status wlg_engine_time_epochs(wlg_engine* engine, uint64_t epochs, wlg_epoch_timing* out);
+/* Launch shape: walkers per CTA of the sweep kernel (1-8) and epochs per CUDA-graph
+ * replay (>= 1); 0 leaves a value unchanged.  No counterpart in the reference. */
+wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block,
+                                 int32_t epochs_per_graph);
 uint64_t wlg_engine_walkers(const wlg_engine* engine);
 uint64_t wlg_engine_bins(const wlg_engine* engine);
 uint64_t wlg_engine_spins(const wlg_engine* engine);

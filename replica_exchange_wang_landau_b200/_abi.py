@@ -126,6 +126,17 @@ class wlg_run_totals(C.Structure):
     ]
 
 
+class wlg_epoch_timing(C.Structure):
+    _fields_ = [
+        ("epochs", C.c_uint64),
+        ("walk_ms", C.c_double),
+        ("exchange_ms", C.c_double),
+        ("total_ms", C.c_double),
+        ("attempted", C.c_uint64),
+        ("accepted", C.c_uint64),
+    ]
+
+
 class wlg_snapshot(C.Structure):
     _fields_ = [
         ("walker_id", C.c_uint64),
@@ -153,6 +164,7 @@ STRUCTS = {
     "wlg_walker_statistics": wlg_walker_statistics,
     "wlg_run_totals": wlg_run_totals,
     "wlg_snapshot": wlg_snapshot,
+    "wlg_epoch_timing": wlg_epoch_timing,
 }
 
 P = C.POINTER
@@ -163,6 +175,7 @@ _vp = C.c_void_p
 SIGNATURES = {
     "wlg_abi_version": (_i32, []),
     "wlg_last_error": (C.c_char_p, []),
+    "wlg_set_device": (_i32, [_i32]),
     "wlg_default_run_config": (_i32, [_u64, P(wlg_run_config)]),
     "wlg_grid_bins": (_i32, [_dbl, _dbl, _dbl, P(_u64)]),
     "wlg_grid_index": (_i32, [_dbl, _dbl, _dbl, _dbl, P(_i64)]),
@@ -178,6 +191,8 @@ SIGNATURES = {
     "wlg_engine_run": (_i32, [_vp, P(wlg_run_totals)]),
     "wlg_engine_run_epochs": (_i32, [_vp, _u64, P(_u64), P(_i32)]),
     "wlg_engine_totals": (_i32, [_vp, P(wlg_run_totals)]),
+    "wlg_engine_time_epochs": (_i32, [_vp, _u64, P(wlg_epoch_timing)]),
+    "wlg_engine_set_launch": (_i32, [_vp, _i32, _i32]),
     "wlg_engine_walkers": (_u64, [_vp]),
     "wlg_engine_bins": (_u64, [_vp]),
     "wlg_engine_spins": (_u64, [_vp]),

@@ -89,6 +89,10 @@ int32_t wlg_abi_version(void) { return WLG_ABI_VERSION; }
 
 const char* wlg_last_error(void) { return g_last_error.c_str(); }
 
+wlg_status wlg_set_device(int32_t device) {
+    return guarded([&] { wlg::check_cuda(cudaSetDevice(device), "cudaSetDevice"); });
+}
+
 wlg_status wlg_default_run_config(uint64_t n, wlg_run_config* out) {
     return guarded([&] {
         if (!out) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null output");
@@ -293,12 +297,15 @@ wlg_status wlg_engine_create(const wlg_system* system, const wlg_run_config* con
 
 void wlg_engine_destroy(wlg_engine* engine) {
     if (!engine) return;
+    if (engine->impl) cudaSetDevice(engine->impl->device);
     delete engine->impl;
     delete engine;
 }
 
 #define WLG_ENGINE_GUARD(engine)                                                                 \
-    if (!(engine) || !(engine)->impl) return fail(WLG_ERR_INVALID_ARGUMENT, "null engine");
+    if (!(engine) || !(engine)->impl) return fail(WLG_ERR_INVALID_ARGUMENT, "null engine");  \
+    if (cudaSetDevice((engine)->impl->device) != cudaSuccess)                                    \
+        return fail(WLG_ERR_DEVICE, "cannot select the engine's CUDA device");
 
 wlg_status wlg_engine_run(wlg_engine* engine, wlg_run_totals* totals) {
     WLG_ENGINE_GUARD(engine)
@@ -313,6 +320,19 @@ wlg_status wlg_engine_run_epochs(wlg_engine* engine, uint64_t max_epochs, uint64
 wlg_status wlg_engine_totals(wlg_engine* engine, wlg_run_totals* totals) {
     WLG_ENGINE_GUARD(engine)
     return guarded([&] { engine->impl->totals(totals); });
+}
+
+wlg_status wlg_engine_time_epochs(wlg_engine* engine, uint64_t epochs, wlg_epoch_timing* out) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] {
+        if (!out) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null output");
+        engine->impl->time_epochs(epochs, out);
+    });
+}
+
+wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block, int32_t epochs_per_graph) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] { engine->impl->set_launch(walkers_per_block, epochs_per_graph); });
 }
 
 uint64_t wlg_engine_walkers(const wlg_engine* engine) { return engine && engine->impl ? engine->impl->walkers() : 0; }

@@ -5,6 +5,7 @@
 // that no multiply-add is contracted (the reference's ISO C++20 x86-64 build has none).
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>

@@ -109,6 +109,7 @@ Engine::Engine(const wlg_system& system, const wlg_run_config& c) : cfg_(c) {
     cfg_.checkpoint_path = nullptr;
 
     require_device();
+    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
     check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
     upload_system(system, sys_, stream_);
     build_couplings(sys_, precision_, stream_);
@@ -481,6 +482,69 @@ void Engine::run_epochs(uint64_t max_epochs, uint64_t* epochs_run, int32_t* done
 void Engine::run(wlg_run_totals* out) {
     while (!done_) run_epochs(~0ULL, nullptr, nullptr);
     if (out) totals(out);
+}
+
+void Engine::time_epochs(uint64_t epochs, wlg_epoch_timing* out) {
+    wlg_run_totals before{}, after{};
+    totals(&before);
+    WalkArgs a{};
+    a.first = 0;
+    a.count = static_cast<int32_t>(walkers_);
+    a.epoch_mode = 1;
+    a.smem_per_walker = static_cast<int32_t>(walker_smem_bytes(view_, smem_fields_, features_));
+    std::vector<cudaEvent_t> ev(3 * epochs + 1);
+    for (auto& e : ev) check_cuda(cudaEventCreate(&e), "cudaEventCreate");
+    uint64_t ran = 0;
+    try {
+        check_cuda(cudaEventRecord(ev[0], stream_), "record");
+        for (uint64_t k = 0; k < epochs && !done_; ++k) {
+            launch_walk(view_, a, walkers_per_block, stream_);
+            check_cuda(cudaEventRecord(ev[3 * k + 1], stream_), "record");
+            launch_exchange(view_, stream_);
+            check_cuda(cudaEventRecord(ev[3 * k + 2], stream_), "record");
+            check_cuda(cudaEventRecord(ev[3 * k + 3], stream_), "record");
+            ++ran;
+        }
+        check_device_error();
+        wlg_epoch_timing t{};
+        t.epochs = ran;
+        for (uint64_t k = 0; k < ran; ++k) {
+            float walk = 0.f, ex = 0.f;
+            check_cuda(cudaEventElapsedTime(&walk, ev[3 * k], ev[3 * k + 1]), "elapsed");
+            check_cuda(cudaEventElapsedTime(&ex, ev[3 * k + 1], ev[3 * k + 2]), "elapsed");
+            t.walk_ms += walk;
+            t.exchange_ms += ex;
+        }
+        float total = 0.f;
+        if (ran) check_cuda(cudaEventElapsedTime(&total, ev[0], ev[3 * ran]), "elapsed");
+        t.total_ms = total;
+        totals(&after);
+        t.attempted = after.attempted - before.attempted;
+        t.accepted = after.accepted - before.accepted;
+        *out = t;
+    } catch (...) {
+        for (auto& e : ev) cudaEventDestroy(e);
+        throw;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+}
+
+void Engine::set_launch(int wpb, int epg) {
+    if (wpb < 0 || wpb > 8 || epg < 0) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "invalid launch shape");
+    if (wpb) walkers_per_block = wpb;
+    if (epg && epg != epochs_per_graph) {
+        epochs_per_graph = epg;
+        if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+        if (graph_) cudaGraphDestroy(graph_);
+        graph_exec_ = nullptr;
+        graph_ = nullptr;
+    }
+    if (wpb && graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+        cudaGraphDestroy(graph_);
+        graph_exec_ = nullptr;
+        graph_ = nullptr;
+    }
 }
 
 void Engine::totals(wlg_run_totals* out) {

@@ -148,6 +148,8 @@ class Engine {
     void run(wlg_run_totals* totals);
     void run_epochs(uint64_t max_epochs, uint64_t* epochs_run, int32_t* done);
     void totals(wlg_run_totals* out);
+    void time_epochs(uint64_t epochs, wlg_epoch_timing* out);
+    void set_launch(int walkers_per_block, int epochs_per_graph);
     uint64_t walkers() const { return walkers_; }
     uint64_t bins() const { return bins_; }
     uint64_t spins() const { return sys_.n; }
@@ -168,6 +170,7 @@ class Engine {
     // Launch shape (chosen by the autotuner or set explicitly).
     int walkers_per_block = 1;
     int epochs_per_graph = 32;
+    int device = 0;  // CUDA device the engine lives on
 
   private:
     void initialise_walkers(const wlg_run_config& c);

@@ -606,6 +606,9 @@ void launch_walk(const EngineView& v, const WalkArgs& a, int wpb, cudaStream_t s
     const bool smem_fields = a.smem_per_walker >= static_cast<int>(walker_smem_bytes(v, true, features));
     WalkFn fn = pick_walk(v.precision, v.csr != 0, smem_fields, features);
     wpb = std::max(1, std::min(wpb, 8));
+    while (wpb > 1 && static_cast<size_t>(a.smem_per_walker) * wpb > 227 * 1024) --wpb;
+    if (static_cast<size_t>(a.smem_per_walker) > 227 * 1024)
+        throw WlgError(WLG_ERR_INVALID_ARGUMENT, "walker state does not fit in shared memory");
     const unsigned blocks = static_cast<unsigned>((a.count + wpb - 1) / wpb);
     fn<<<blocks, 32 * wpb, static_cast<size_t>(a.smem_per_walker) * wpb, stream>>>(v, a);
     check_cuda(cudaGetLastError(), "walk_kernel");
@@ -616,6 +619,9 @@ void launch_init(const EngineView& v, const InitArgs& a, int wpb, cudaStream_t s
     const bool smem_fields = a.smem_per_walker >= static_cast<int>(walker_smem_bytes(v, true, features));
     InitFn fn = pick_init(v.csr != 0, smem_fields, features);
     wpb = std::max(1, std::min(wpb, 8));
+    while (wpb > 1 && static_cast<size_t>(a.smem_per_walker) * wpb > 227 * 1024) --wpb;
+    if (static_cast<size_t>(a.smem_per_walker) > 227 * 1024)
+        throw WlgError(WLG_ERR_INVALID_ARGUMENT, "walker state does not fit in shared memory");
     const unsigned blocks = static_cast<unsigned>((v.walkers + wpb - 1) / wpb);
     fn<<<blocks, 32 * wpb, static_cast<size_t>(a.smem_per_walker) * wpb, stream>>>(v, a);
     check_cuda(cudaGetLastError(), "init_kernel");

@@ -500,6 +500,8 @@ class Engine:
         self._h = handle
         self.n = n
         self.bins = int(self._lib.wlg_engine_bins(self._h))
+        if walkers_per_block:
+            self.set_launch(walkers_per_block, 0)
         self.walkers = int(self._lib.wlg_engine_walkers(self._h))
 
     def close(self) -> None:
@@ -529,6 +531,15 @@ class Engine:
         ran, done = C.c_uint64(0), C.c_int32(0)
         _check(self._lib.wlg_engine_run_epochs(self._h, int(epochs), C.byref(ran), C.byref(done)))
         return int(ran.value), bool(done.value)
+
+    def time_epochs(self, epochs: int) -> dict:
+        """Runs `epochs` epochs with CUDA events around every kernel (device time, ms)."""
+        t = _abi.wlg_epoch_timing()
+        _check(self._lib.wlg_engine_time_epochs(self._h, int(epochs), C.byref(t)))
+        return {name: getattr(t, name) for name, _ in _abi.wlg_epoch_timing._fields_}
+
+    def set_launch(self, walkers_per_block: int = 0, epochs_per_graph: int = 0) -> None:
+        _check(self._lib.wlg_engine_set_launch(self._h, int(walkers_per_block), int(epochs_per_graph)))
 
     def totals(self) -> dict:
         t = _abi.wlg_run_totals()
@@ -634,6 +645,11 @@ def run_rewl(system: System, config: RunConfig, walkers_per_block: int | None = 
 
 
 # ---- host helpers ---------------------------------------------------------------------
+
+
+def set_device(device: int) -> None:
+    """Selects the CUDA device for engines created afterwards on this thread."""
+    _check(load_library().wlg_set_device(int(device)))
 
 
 def grid_bins(emin: float, emax: float, width: float) -> int:

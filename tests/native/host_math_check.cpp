@@ -1,0 +1,53 @@
+// Host-side check of two exact integer routines the kernels use (csrc/common.cuh):
+//  * x87_mean(total, count) must equal (double)((long double)total / (long double)count),
+//    the reference's histogram mean (src/wang_landau.cpp:349-361);
+//  * fast_mod(x) must equal x % bound (Barrett reduction used by bounded(),
+//    include/wl/rng.hpp:29-36).
+// Prints "ok <cases>" or the first mismatch.
+#include <cinttypes>
+#include <cstdio>
+#include <cstring>
+
+#include "../../replica_exchange_wang_landau_b200/csrc/common.cuh"
+
+int main() {
+    wlg::Rng rng;
+    rng.seed(2024, 7);
+    uint64_t cases = 0;
+    for (int k = 0; k < 3000000; ++k) {
+        const uint64_t a = 1 + rng.next() % (k % 3 == 0 ? 4096 : (k % 3 == 1 ? 64 : 1000000007ULL));
+        uint64_t t = rng.next();
+        switch (k % 5) {
+            case 0: t %= 1000; break;
+            case 1: t %= 1ULL << 40; break;
+            case 2: t = (t % 100000) * a + (rng.next() % a); break;
+            case 3: t >>= (rng.next() % 64); break;
+            default: break;
+        }
+        const double want = static_cast<double>(static_cast<long double>(t) / static_cast<long double>(a));
+        const double got = wlg::x87_mean(t, a);
+        if (t != 0 && std::memcmp(&want, &got, 8) != 0) {
+            std::printf("x87_mean mismatch total=%" PRIu64 " count=%" PRIu64 " want=%a got=%a\n", t, a, want, got);
+            return 1;
+        }
+        ++cases;
+    }
+    const uint64_t bounds[] = {1, 2, 3, 7, 8, 27, 100, 512, 2458, 32768, 1000003, 2147483647ULL};
+    for (uint64_t b : bounds) {
+        const wlg::FastMod f = wlg::make_fastmod(b);
+        for (int k = 0; k < 200000; ++k) {
+            const uint64_t x = k < 10 ? ~0ULL - static_cast<uint64_t>(k) : rng.next();
+            if (wlg::fast_mod(f, x) != x % b) {
+                std::printf("fast_mod mismatch x=%" PRIu64 " bound=%" PRIu64 "\n", x, b);
+                return 1;
+            }
+            ++cases;
+        }
+        if (f.threshold != (0ULL - b) % b) {
+            std::printf("threshold mismatch bound=%" PRIu64 "\n", b);
+            return 1;
+        }
+    }
+    std::printf("ok %" PRIu64 "\n", cases);
+    return 0;
+}
