@@ -163,6 +163,13 @@ class Oracle(_Checker):
         self.lib.orc_couplings_destroy(h)
         return out
 
+    def csr_nnz(self, system: System) -> int:
+        """Number of stored couplings (CSR) of the restated CsrCouplings."""
+        h = self._couplings(system)
+        nnz = int(self.lib.orc_couplings_nnz(h))
+        self.lib.orc_couplings_destroy(h)
+        return nnz
+
     def local_fields(self, system: System, spins: np.ndarray):
         h = self._couplings(system)
         s = np.ascontiguousarray(spins, dtype=np.int8).reshape(-1, system.size())

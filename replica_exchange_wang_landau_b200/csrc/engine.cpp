@@ -149,8 +149,8 @@ void Engine::initialise_walkers(const wlg_run_config& c) {
     zeroed(d_hist_, W * B * sizeof(uint64_t));
     zeroed(d_active_, W * B);
     zeroed(d_refine_, features_ ? W * B : 16);
-    zeroed(d_sqdisp_, p_.collect ? W * B * sizeof(double) : 16);
-    zeroed(d_dsamples_, p_.collect ? W * B * sizeof(uint64_t) : 16);
+    zeroed(d_sqdisp_, features_ ? W * B * sizeof(double) : 16);
+    zeroed(d_dsamples_, features_ ? W * B * sizeof(uint64_t) : 16);
     zeroed(d_spins_, W * ld);
     zeroed(d_fields_, W * ld * sizeof(double));
     const uint64_t R = p_.collect ? W * kRepresentatives : 1;

@@ -214,8 +214,10 @@ __global__ void __launch_bounds__(256) walk_kernel(EngineView v, WalkArgs a) {
         act_s[b] = v.active[boff + b];
         if constexpr (kFeat) {
             ref_s[b] = v.refine[boff + b];
-            sq_s[b] = v.sqdisp[boff + b];
-            ds_s[b] = v.dsamples[boff + b];
+            if (collect) {  // the pilot arrays exist only in pilot runs
+                sq_s[b] = v.sqdisp[boff + b];
+                ds_s[b] = v.dsamples[boff + b];
+            }
         }
     }
     __syncwarp();
@@ -381,8 +383,10 @@ __global__ void __launch_bounds__(256) walk_kernel(EngineView v, WalkArgs a) {
         v.active[boff + b] = act_s[b];
         if constexpr (kFeat) {
             v.refine[boff + b] = ref_s[b];
-            v.sqdisp[boff + b] = sq_s[b];
-            v.dsamples[boff + b] = ds_s[b];
+            if (collect) {
+                v.sqdisp[boff + b] = sq_s[b];
+                v.dsamples[boff + b] = ds_s[b];
+            }
         }
     }
     if (lane == 0) {
