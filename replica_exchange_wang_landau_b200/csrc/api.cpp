@@ -135,7 +135,7 @@ wlg_status wlg_grid_bins(double emin, double emax, double width, uint64_t* bins)
 wlg_status wlg_grid_index(double emin, double emax, double width, double energy, int64_t* bin) {
     return guarded([&] {
         const uint64_t count = wlg::grid_bins(emin, emax, width);
-        *bin = wlg::grid_index(wlg::Grid{emin, emax, width, static_cast<int64_t>(count)}, energy);
+        *bin = wlg::grid_index(wlg::make_grid(emin, emax, width, static_cast<int64_t>(count)), energy);
     });
 }
 

@@ -60,6 +60,9 @@ struct FastMod {
     uint64_t bound;
     uint64_t m;
     uint64_t threshold;  // (-bound) % bound, the rejection threshold of bounded()
+    uint64_t mask;       // bound - 1 when bound is a power of two (x % bound == x & mask)
+    int32_t pow2;
+    int32_t pad;
 };
 
 inline FastMod make_fastmod(uint64_t bound) {
@@ -67,6 +70,9 @@ inline FastMod make_fastmod(uint64_t bound) {
     f.bound = bound;
     f.m = bound ? (~0ULL) / bound : 0;
     f.threshold = bound ? (0ULL - bound) % bound : 0;
+    f.pow2 = bound != 0 && (bound & (bound - 1)) == 0;
+    f.mask = bound ? bound - 1 : 0;
+    f.pad = 0;
     return f;
 }
 
@@ -79,6 +85,7 @@ WLG_HD uint64_t mulhi64(uint64_t a, uint64_t b) {
 }
 
 WLG_HD uint64_t fast_mod(const FastMod& f, uint64_t x) {
+    if (f.pow2) return x & f.mask;  // threshold is 0: no draw is ever rejected
     uint64_t r = x - mulhi64(x, f.m) * f.bound;
     if (r >= f.bound) r -= f.bound;
     if (r >= f.bound) r -= f.bound;
@@ -99,14 +106,28 @@ struct Grid {
     double minimum;
     double maximum;
     double width;
-    int64_t count;  // llround((maximum - minimum) / width)
+    int64_t count;       // llround((maximum - minimum) / width)
+    double inv_width;    // 1 / width, exact when width is a power of two
+    int32_t pow2_width;  // width is a power of two: x / width == x * inv_width exactly
+    int32_t pad;
 };
 
+inline Grid make_grid(double minimum, double maximum, double width, int64_t count) {
+    Grid g{minimum, maximum, width, count, 1.0 / width, 0, 0};
+    int exponent = 0;
+    g.pow2_width = std::frexp(width, &exponent) == 0.5 ? 1 : 0;
+    return g;
+}
+
 // EnergyGrid::index; -1 for std::nullopt.  `!(e >= min && e <= max)` also rejects NaN
-// and infinities, which is what `!isfinite(e) || e < min || e > max` does.
+// and infinities, which is what `!isfinite(e) || e < min || e > max` does.  Dividing by a
+// power-of-two width and multiplying by its (exact) reciprocal give the same rounded
+// value, so the multiply is used whenever the width allows it.
 WLG_HD int64_t grid_index(const Grid& g, double e) {
     if (!(e >= g.minimum && e <= g.maximum)) return -1;
-    uint64_t raw = static_cast<uint64_t>(floor((e - g.minimum) / g.width));
+    const double offset = e - g.minimum;
+    const double q = g.pow2_width ? offset * g.inv_width : offset / g.width;
+    uint64_t raw = static_cast<uint64_t>(floor(q));
     if (raw == static_cast<uint64_t>(g.count) && e == g.maximum) raw = static_cast<uint64_t>(g.count) - 1;
     if (raw >= static_cast<uint64_t>(g.count)) return -1;
     return static_cast<int64_t>(raw);

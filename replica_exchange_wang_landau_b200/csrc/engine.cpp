@@ -87,7 +87,7 @@ Engine::Engine(const wlg_system& system, const wlg_run_config& c) : cfg_(c) {
     wpw_ = c.walkers_per_window;
     walkers_ = windows_ * wpw_;
     precision_ = c.coupling_precision;
-    grid_ = Grid{c.emin, c.emax, c.bin_width, static_cast<int64_t>(bins_)};
+    grid_ = make_grid(c.emin, c.emax, c.bin_width, static_cast<int64_t>(bins_));
     features_ = c.wl.collect_window_statistics != 0 || c.wl.nalivaiko_mod != 0;
 
     p_.flatness = c.wl.flatness;

@@ -12,6 +12,21 @@ namespace wlg {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// The acceptance test of attempt_flip and of the initialisation search,
+// log(max(u, 2^-53)) < threshold (src/wang_landau.cpp:207-208, 261), with the same result
+// as evaluating it with the full-precision log().  A one-instruction log2 estimate (MUFU)
+// decides whenever it is farther than 1e-3 from the threshold: for u' in [2^-53, 1) its
+// error, including the rounding of u' to float and of the product by ln 2, is below 1e-5,
+// and log() itself is within one ulp, so the comparison cannot flip.  Only the ~0.1% of
+// draws inside the margin pay for log().
+__device__ __forceinline__ bool log_uniform_below(double u, double threshold) {
+    const double up = fmax(u, 0x1.0p-53);
+    const double estimate = static_cast<double>(__log2f(static_cast<float>(up))) * 0.6931471805599453;
+    if (estimate < threshold - 1e-3) return true;
+    if (estimate > threshold + 1e-3) return false;
+    return log(up) < threshold;
+}
+
 __device__ __forceinline__ uint64_t warp_sum_u64(uint64_t x) {
 #pragma unroll
     for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
