@@ -224,6 +224,18 @@ wlg_status wlg_couplings_csr(const wlg_system* system, uint64_t* nnz, uint64_t* 
  * (count x n spins), computed with the reference's summation order. */
 wlg_status wlg_local_fields(const wlg_system* system, const int8_t* spins, uint64_t count,
                             double* fields, double* energies);
+/* The same results as wlg_local_fields for callers that cannot allocate device memory (a
+ * host whose own pool already holds the GPU's memory, code that must not add the device
+ * synchronisation cudaMalloc/cudaFree can cause, hosts that forbid allocation after
+ * start-up).  No counterpart in the reference.  Nothing is allocated: the couplings and all
+ * staging live in one static device array of 18 MiB that every GPU loading this library
+ * keeps until the process exits.  Limits: dense systems only (cutoff 0), n <= 1024 sites,
+ * count <= 65536 configurations and count * n <= 1048576; larger inputs return
+ * WLG_ERR_INVALID_ARGUMENT with the limit in the message.  The first call on a device looks
+ * up the array's device address and should come before any stream capture.  Calls share
+ * the array: calls that overlap on the GPU race. */
+wlg_status wlg_local_fields_noalloc(const wlg_system* system, const int8_t* spins,
+                                    uint64_t count, double* fields, double* energies);
 
 /* ---- the REWL engine: run_rewl (src/parallel.cpp:276-747) ---------------------- */
 

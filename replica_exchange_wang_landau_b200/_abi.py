@@ -186,6 +186,7 @@ SIGNATURES = {
     "wlg_couplings_dense": (_i32, [P(wlg_system), _i32, P(_dbl)]),
     "wlg_couplings_csr": (_i32, [P(wlg_system), P(_u64), P(_u64), P(_u64), P(_dbl)]),
     "wlg_local_fields": (_i32, [P(wlg_system), P(C.c_int8), _u64, P(_dbl), P(_dbl)]),
+    "wlg_local_fields_noalloc": (_i32, [P(wlg_system), P(C.c_int8), _u64, P(_dbl), P(_dbl)]),
     "wlg_engine_create": (_i32, [P(wlg_system), P(wlg_run_config), P(_vp)]),
     "wlg_engine_destroy": (None, [_vp]),
     "wlg_engine_run": (_i32, [_vp, P(wlg_run_totals)]),

@@ -286,6 +286,14 @@ wlg_status wlg_local_fields(const wlg_system* system, const int8_t* spins, uint6
     });
 }
 
+wlg_status wlg_local_fields_noalloc(const wlg_system* system, const int8_t* spins, uint64_t count, double* fields,
+                                    double* energies) {
+    return guarded([&] {
+        if (!system || !spins || !fields) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        wlg::local_fields_noalloc(*system, spins, count, fields, energies);
+    });
+}
+
 wlg_status wlg_engine_create(const wlg_system* system, const wlg_run_config* config, wlg_engine** engine) {
     return guarded([&] {
         if (!system || !config || !engine) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");

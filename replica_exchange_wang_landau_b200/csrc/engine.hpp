@@ -77,6 +77,12 @@ bool load_checkpoint_file(const std::string& path, std::vector<int8_t>& spins, s
 
 // physics.cu
 void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream);
+// noalloc.cu: local fields with every intermediate in a static device array.
+void local_fields_noalloc(const wlg_system& s, const int8_t* spins, uint64_t count, double* fields,
+                          double* energies);
+// dense_build_kernel on caller-provided device buffers (J is ld x ld and must be zeroed).
+void launch_dense_build(const double* pos, const double* axes, const double* box, int periodic, double scale, int n,
+                        int ld, double* J, int* err, cudaStream_t stream);
 void compute_fields(const EngineView& v, const int8_t* spins, int64_t spin_stride, double* fields,
                     int64_t field_stride, double* energies, int count, cudaStream_t stream);
 

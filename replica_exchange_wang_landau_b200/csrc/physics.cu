@@ -192,6 +192,21 @@ static SystemView make_view(const DeviceSystem& d) {
     return s;
 }
 
+void launch_dense_build(const double* pos, const double* axes, const double* box, int periodic, double scale, int n,
+                        int ld, double* J, int* err, cudaStream_t stream) {
+    SystemView s;
+    s.pos = pos;
+    s.axes = axes;
+    for (int k = 0; k < 3; ++k) s.box[k] = box[k];
+    s.periodic = periodic;
+    s.scale = scale;
+    s.cutoff = 0.0;
+    s.n = n;
+    const int tiles = (ld + 31) / 32;
+    dense_build_kernel<<<dim3(tiles, tiles), dim3(32, 8), 0, stream>>>(s, ld, J, err);
+    check_cuda(cudaGetLastError(), "dense_build_kernel");
+}
+
 void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream) {
     const SystemView s = make_view(d);
     DeviceBuffer err(sizeof(int));
