@@ -50,6 +50,23 @@ struct Rng {
     }
 };
 
+// The inverse of Rng::next()'s state transition (the transition is an invertible linear map
+// over GF(2)).  A sweep that generates draws ahead of their use rewinds its state by the
+// number of unused draws, so the state it stores is the one after the consumed draws.
+WLG_HD void rng_step_back(Rng& r) {
+    // forward: a2 = s2^s0, a3 = s3^s1, a1 = s1^a2, a0 = s0^a3, b2 = a2^(s1<<17), b3 = rotl(a3,45)
+    const uint64_t a3 = (r.s3 >> 45) | (r.s3 << 19);  // rotr(b3, 45)
+    const uint64_t s0 = r.s0 ^ a3;
+    // a1 ^ b2 = s1 ^ (s1 << 17); invert x ^ (x << 17)
+    const uint64_t y = r.s1 ^ r.s2;
+    const uint64_t s1 = y ^ (y << 17) ^ (y << 34) ^ (y << 51);
+    const uint64_t a2 = r.s2 ^ (s1 << 17);
+    r.s0 = s0;
+    r.s1 = s1;
+    r.s2 = a2 ^ s0;
+    r.s3 = a3 ^ s1;
+}
+
 // uniform(): rng.hpp:25-27 — exact for the 53-bit integer.
 WLG_HD double to_uniform(uint64_t x) { return static_cast<double>(x >> 11) * 0x1.0p-53; }
 

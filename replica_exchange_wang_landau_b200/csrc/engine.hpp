@@ -130,6 +130,8 @@ size_t walker_smem_bytes(const EngineView& v, bool smem_fields, bool features);
 bool fields_fit_in_smem(const EngineView& v, bool features);
 void launch_init(const EngineView& v, const InitArgs& a, int walkers_per_block, cudaStream_t stream);
 void launch_walk(const EngineView& v, const WalkArgs& a, int walkers_per_block, cudaStream_t stream);
+// sweep.cu: the dense sweep; false when the walker does not fit the shared-memory ring.
+bool launch_sweep_dense(const EngineView& v, const WalkArgs& a, cudaStream_t stream);
 void launch_exchange(const EngineView& v, cudaStream_t stream);
 void launch_flush_pending(const EngineView& v, cudaStream_t stream);
 void launch_summarize(const EngineView& v, int window, int allow_empty, double* log_g, uint64_t* hist,

@@ -1,0 +1,479 @@
+// sweep.cu — the dense REWL sweep: WangLandauWalker::run_attempts / attempt_flip
+// (src/wang_landau.cpp:244-315) for one batch of exchange_interval attempts, then the
+// walker-local flatness / 1/t check of run_rewl (src/parallel.cpp:395-407).
+//
+// One warp owns one walker (one CTA per walker: with 128 walkers on 148 SMs every walker has
+// an SM to itself).  The walker's local fields, spins and window slice of log_g / H / active
+// live in shared memory, and the J rows it will need arrive in a shared-memory ring ahead of
+// time:
+//
+// * The random site of an attempt is the next unconsumed draw of the walker's xoshiro
+//   stream, whatever the walk did before, so the warp generates its draws kSlots ahead and,
+//   for every draw, starts a bulk asynchronous copy (cp.async.bulk, completion counted on an
+//   mbarrier) of the J row of the site that draw would select.  A draw consumed as a site
+//   whose flip is accepted finds its row on chip; a draw consumed as the acceptance uniform
+//   just frees its slot.  At the end of the batch the generator is stepped back over the
+//   draws still queued (rng_step_back), so the stored RNG state is the reference's.
+// * All 32 lanes evaluate the scalar decision chain redundantly (identical registers, no
+//   shuffles); the lanes split the N-element field update.  One elected lane issues the
+//   copies (elect.sync, no branch).
+// * Every mbarrier wait is bounded; on timeout the walker records WLG_ERR_TIMEOUT, drains its
+//   outstanding copies (bounded again) and returns without writing its state back.
+//
+// The arithmetic is the reference's, operation for operation (see walker.cu for the shared
+// argument about fma(m, J, h) with m = +-2 and the power-of-two bin width).
+#include "engine.hpp"
+#include "walker_dev.cuh"
+
+namespace wlg {
+
+namespace {
+
+constexpr int kSlots = 4;
+constexpr uint32_t kWaitPolls = 1u << 18;
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Warp-uniform bounded wait for the completion of phase `parity` of one barrier.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    if (__all_sync(kFull, mbar_try(bar, parity))) return true;
+    for (uint32_t k = 1; k < kWaitPolls; ++k)
+        if (__all_sync(kFull, mbar_try(bar, parity))) return true;
+    return false;
+}
+// One elected lane arms the slot's barrier with the row size and starts the row copy.
+// `fence` orders this warp's earlier shared-memory reads of the slot before the copy.
+__device__ __forceinline__ void issue_row(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar, bool fence) {
+    if (fence) {
+        asm volatile(
+            "{\n .reg .pred p;\n elect.sync _|p, 0xffffffff;\n"
+            " @p fence.proxy.async.shared::cta;\n"
+            " @p mbarrier.arrive.expect_tx.shared::cta.b64 _, [%3], %2;\n"
+            " @p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n}" ::"r"(dst),
+            "l"(src), "r"(bytes), "r"(bar)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n .reg .pred p;\n elect.sync _|p, 0xffffffff;\n"
+            " @p mbarrier.arrive.expect_tx.shared::cta.b64 _, [%3], %2;\n"
+            " @p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n}" ::"r"(dst),
+            "l"(src), "r"(bytes), "r"(bar)
+            : "memory");
+    }
+}
+
+struct RingLayout {
+    size_t ring, bars, base, total;
+};
+__host__ __device__ inline RingLayout ring_layout(int ld, int mwb, bool features, size_t jbytes) {
+    RingLayout L;
+    size_t at = 0;
+    L.ring = at;
+    at += kSlots * round16(static_cast<size_t>(ld) * jbytes);
+    L.bars = at;
+    at += round16(kSlots * 8);
+    L.base = at;
+    at += smem_layout(ld, mwb, true, features).total;
+    L.total = at;
+    return L;
+}
+
+template <int kPrec> struct CouplingType;
+template <> struct CouplingType<WLG_PRECISION_FP64> { using T = double; };
+template <> struct CouplingType<WLG_PRECISION_FP32> { using T = float; };
+template <> struct CouplingType<WLG_PRECISION_BF16> { using T = __nv_bfloat16; };
+
+// fields[j] += m * row[j] (add_flip_delta, src/physics.cpp:190-195) from a row in shared
+// memory; m * row[j] is exact (m = +-2, times the BF16 row scale), so fma rounds once as
+// the reference's multiply-then-add does.
+template <int kPrec>
+__device__ __forceinline__ void row_update(const void* row_smem, int ld, double m, double* f, int lane) {
+    double2* f2 = reinterpret_cast<double2*>(f);
+    if constexpr (kPrec == WLG_PRECISION_FP64) {
+        const double2* r = reinterpret_cast<const double2*>(row_smem);
+#pragma unroll 4
+        for (int k = lane; k < (ld >> 1); k += 32) {
+            const double2 a = r[k];
+            double2 h = f2[k];
+            h.x = fma(m, a.x, h.x);
+            h.y = fma(m, a.y, h.y);
+            f2[k] = h;
+        }
+    } else if constexpr (kPrec == WLG_PRECISION_FP32) {
+        const float4* r = reinterpret_cast<const float4*>(row_smem);
+#pragma unroll 2
+        for (int k = lane; k < (ld >> 2); k += 32) {
+            const float4 a = r[k];
+            double2 h0 = f2[2 * k], h1 = f2[2 * k + 1];
+            h0.x = fma(m, static_cast<double>(a.x), h0.x);
+            h0.y = fma(m, static_cast<double>(a.y), h0.y);
+            h1.x = fma(m, static_cast<double>(a.z), h1.x);
+            h1.y = fma(m, static_cast<double>(a.w), h1.y);
+            f2[2 * k] = h0;
+            f2[2 * k + 1] = h1;
+        }
+    } else {
+        const uint4* r = reinterpret_cast<const uint4*>(row_smem);
+        for (int k = lane; k < (ld >> 3); k += 32) {
+            const uint4 raw = r[k];
+            const uint32_t words[4] = {raw.x, raw.y, raw.z, raw.w};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                double2 h = f2[4 * k + q];
+                h.x = fma(m, static_cast<double>(__uint_as_float(words[q] << 16)), h.x);
+                h.y = fma(m, static_cast<double>(__uint_as_float(words[q] & 0xffff0000u)), h.y);
+                f2[4 * k + q] = h;
+            }
+        }
+    }
+}
+
+template <int kPrec, bool kFeat>
+__global__ void __launch_bounds__(32, 1) sweep_dense_kernel(EngineView v, WalkArgs a) {
+    using JT = typename CouplingType<kPrec>::T;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    if (static_cast<int>(blockIdx.x) >= a.count) return;
+    const int w = a.first + static_cast<int>(blockIdx.x);
+    Control* ctl = v.ctl;
+    if (a.epoch_mode && *reinterpret_cast<volatile int32_t*>(&ctl->done)) return;
+
+    const RingLayout RL = ring_layout(v.ld, v.max_window_bins, kFeat, sizeof(JT));
+    const SmemLayout L = smem_layout(v.ld, v.max_window_bins, true, kFeat);
+    unsigned char* base = smem + RL.base;
+    const JT* ring_rows = reinterpret_cast<const JT*>(smem + RL.ring);
+    double* f = reinterpret_cast<double*>(base + L.fields);
+    double* lg_s = reinterpret_cast<double*>(base + L.log_g);
+    uint64_t* h_s = reinterpret_cast<uint64_t*>(base + L.hist);
+    double* sq_s = reinterpret_cast<double*>(base + L.sq);
+    uint64_t* ds_s = reinterpret_cast<uint64_t*>(base + L.ds);
+    int8_t* sp_s = reinterpret_cast<int8_t*>(base + L.spins);
+    uint8_t* act_s = base + L.active;
+    uint8_t* ref_s = base + L.refine;
+
+    WalkerState st = v.ws[w];
+    const int wb = v.win_begin[st.window], we = v.win_end[st.window], nbins = we - wb;
+    const size_t boff = static_cast<size_t>(w) * static_cast<size_t>(v.grid.count) + static_cast<size_t>(wb);
+    double* fg = v.fields + static_cast<size_t>(st.slot) * v.ld;
+    int8_t* sg = v.spins + static_cast<size_t>(st.slot) * v.ld;
+    const DeviceParams& P = v.p;
+    const bool collect = kFeat && P.collect;
+    const bool nalivaiko = kFeat && P.nalivaiko;
+
+    if (st.cur_bin < wb || st.cur_bin >= we) {  // "Walker escaped its energy window"
+        if (lane == 0) record_error(ctl, WLG_ERR_ESCAPED, w);
+        return;
+    }
+    uint32_t batch;
+    {
+        uint64_t b = a.fixed_batch ? a.fixed_batch : P.exchange_interval;
+        if (!a.fixed_batch && P.max_attempts) {
+            const uint64_t remaining = st.attempted < P.max_attempts ? P.max_attempts - st.attempted : 0;
+            b = remaining < b ? remaining : b;
+        }
+        batch = static_cast<uint32_t>(b < 0xffffffffULL ? b : 0xffffffffULL);
+    }
+
+    // ---- the row ring: barriers, then the first kSlots draws and their rows -------------
+    const JT* J = kPrec == WLG_PRECISION_FP64   ? reinterpret_cast<const JT*>(v.J64)
+                  : kPrec == WLG_PRECISION_FP32 ? reinterpret_cast<const JT*>(v.J32)
+                                                : reinterpret_cast<const JT*>(v.J16);
+    const uint32_t row_bytes = static_cast<uint32_t>(v.ld * sizeof(JT));
+    const uint32_t ring_addr = smem_addr(smem + RL.ring);
+    const uint32_t bar_addr = smem_addr(smem + RL.bars);
+    if (lane == 0) {
+        for (int s = 0; s < kSlots; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_addr + 8 * s) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};  // runs kSlots draws ahead of the walk
+    uint64_t q0 = rng.next(), q1 = rng.next(), q2 = rng.next(), q3 = rng.next();
+    issue_row(ring_addr + 0 * row_bytes, J + fast_mod(v.site_mod, q0) * v.ld, row_bytes, bar_addr + 0, false);
+    issue_row(ring_addr + 1 * row_bytes, J + fast_mod(v.site_mod, q1) * v.ld, row_bytes, bar_addr + 8, false);
+    issue_row(ring_addr + 2 * row_bytes, J + fast_mod(v.site_mod, q2) * v.ld, row_bytes, bar_addr + 16, false);
+    issue_row(ring_addr + 3 * row_bytes, J + fast_mod(v.site_mod, q3) * v.ld, row_bytes, bar_addr + 24, false);
+    uint32_t parity = 0;     // bit s: the phase parity the next wait on slot s expects
+    uint32_t inflight = 0xF; // bit s: a copy into slot s has not been observed complete
+    uint32_t head = 0;       // slot holding the row of q0
+    bool failed = false;
+
+    auto wait_slot = [&](uint32_t s) -> bool {
+        if (!((inflight >> s) & 1u)) return true;
+        if (!mbar_wait(bar_addr + 8 * s, (parity >> s) & 1u)) return false;
+        inflight &= ~(1u << s);
+        parity ^= 1u << s;
+        return true;
+    };
+    // consume q0: its slot receives the row for the draw kSlots ahead
+    auto advance = [&](bool fence) {
+        if (!wait_slot(head)) {
+            failed = true;
+            return;
+        }
+        q0 = q1;
+        q1 = q2;
+        q2 = q3;
+        q3 = rng.next();
+        issue_row(ring_addr + head * row_bytes, J + fast_mod(v.site_mod, q3) * v.ld, row_bytes, bar_addr + 8 * head,
+                  fence);
+        inflight |= 1u << head;
+        head = (head + 1) & (kSlots - 1);
+    };
+
+    // ---- stage the walker into shared memory (overlaps the first copies) --------------
+    {
+        const double2* src = reinterpret_cast<const double2*>(fg);
+        double2* dst = reinterpret_cast<double2*>(f);
+        for (int k = lane; k < (v.ld >> 1); k += 32) dst[k] = src[k];
+        const int4* ssrc = reinterpret_cast<const int4*>(sg);
+        int4* sdst = reinterpret_cast<int4*>(sp_s);
+        for (int k = lane; k < (v.ld >> 4); k += 32) sdst[k] = ssrc[k];
+    }
+    for (int b = lane; b < nbins; b += 32) {
+        lg_s[b] = v.log_g[boff + b];
+        h_s[b] = v.hist[boff + b];
+        act_s[b] = v.active[boff + b];
+        if constexpr (kFeat) {
+            ref_s[b] = v.refine[boff + b];
+            if (collect) {
+                sq_s[b] = v.sqdisp[boff + b];
+                ds_s[b] = v.dsamples[boff + b];
+            }
+        }
+    }
+    __syncwarp();
+    if (collect && st.rep_pending) {
+        warp_update_representatives(v, w, st.energy, sp_s, lane);
+        st.rep_pending = 0;
+    }
+
+    // ---- the walk -----------------------------------------------------------------------
+    double E = st.energy;
+    double factor = st.factor;
+    int32_t stage = st.stage;
+    const uint64_t att0 = st.attempted;
+    uint64_t since = st.attempted - st.last_accepted;  // attempted - last_accepted_attempt
+    uint32_t n_acc = 0, n_forced = 0;
+    uint64_t active_count = st.active_count, refine_count = st.refine_count;
+    int32_t rt_state = st.rt_state;
+    uint64_t trips = st.round_trips;
+    const double lower = window_lower(v, wb);
+    const double upper = window_lower(v, we);
+    const Grid g = v.grid;
+    const int gcount = static_cast<int>(g.count);
+    int cur = st.cur_bin;
+    double lg_cur = lg_s[cur - wb];
+    uint64_t hc_cur = h_s[cur - wb];
+    bool act_cur = act_s[cur - wb] != 0;
+    bool ref_cur = nalivaiko ? ref_s[cur - wb] != 0 : true;
+    const uint64_t threshold = v.site_mod.threshold;
+
+    for (uint32_t t = 0; t < batch && !failed;) {
+        if (q0 < threshold) {  // bounded() rejects this draw; the next one is the site
+            advance(false);
+            continue;
+        }
+        const int i = static_cast<int>(fast_mod(v.site_mod, q0));
+        const uint32_t slot = head;
+        const int8_t si = sp_s[i];
+        const double m = -2.0 * static_cast<double>(si);
+        const double delta = m * f[i];  // flip_delta: -2 s_i h_i, exact
+        const double Ep = E + delta;
+        // EnergyGrid::index restricted to the window: -1 when outside the grid
+        int nb = -1;
+        if (Ep >= g.minimum && Ep <= g.maximum) {
+            const double off = Ep - g.minimum;
+            nb = static_cast<int>(floor(g.pow2_width ? off * g.inv_width : off / g.width));
+            if (nb == gcount && Ep == g.maximum) nb = gcount - 1;
+        }
+        const bool in_window = nb >= wb && nb < we;
+        const int li = in_window ? nb - wb : 0;
+        const double lg_new = nb == cur ? lg_cur : lg_s[li];
+        const double log_ratio = lg_cur - lg_new;
+        bool accepted = false, forced = false, used_uniform = false;
+        if (in_window) {
+            if (log_ratio >= 0.0) {
+                accepted = true;
+            } else if (P.force_after != 0 && since >= P.force_after) {
+                accepted = forced = true;
+            } else {
+                used_uniform = true;
+                accepted = log_uniform_below(to_uniform(q1), log_ratio);
+            }
+        }
+        if (accepted) {
+            double mm = m;
+            if constexpr (kPrec == WLG_PRECISION_BF16) mm *= static_cast<double>(__ldg(v.Jscale + i));
+            if (!wait_slot(slot)) {
+                failed = true;
+                break;
+            }
+            row_update<kPrec>(ring_rows + static_cast<size_t>(slot) * v.ld, v.ld, mm, f, lane);
+            if (lane == 0) sp_s[i] = static_cast<int8_t>(-si);
+            E = Ep;
+            ++n_acc;
+            n_forced += forced ? 1u : 0u;
+            since = 0;
+            __syncwarp();  // every lane's reads of the row precede the fenced refill
+        } else {
+            ++since;
+        }
+        advance(accepted);                 // the site draw
+        if (used_uniform) advance(false);  // the acceptance uniform
+        if (collect && lane == 0) {
+            const double displacement = accepted ? delta : 0.0;
+            sq_s[cur - wb] += displacement * displacement;
+            ++ds_s[cur - wb];
+        }
+        ++t;
+        if (stage == kInverseTime) {  // update_inverse_time_factor
+            if (active_count != 0)
+                factor = static_cast<double>(active_count) / static_cast<double>(att0 + t);
+            if (factor <= P.final_factor) stage = kFrozen;
+        }
+        if (accepted && nb != cur) {  // update_current_bin moves to the new bin
+            if (lane == 0) {
+                lg_s[cur - wb] = lg_cur;
+                h_s[cur - wb] = hc_cur;
+                act_s[cur - wb] = act_cur ? 1 : 0;
+                if (nalivaiko) ref_s[cur - wb] = ref_cur ? 1 : 0;
+            }
+            cur = nb;
+            lg_cur = lg_new;
+            hc_cur = h_s[li];
+            act_cur = act_s[li] != 0;
+            ref_cur = nalivaiko ? ref_s[li] != 0 : true;
+        }
+        ++hc_cur;
+        if (!act_cur) {
+            act_cur = true;
+            ++active_count;
+        }
+        if (nalivaiko && !ref_cur) {
+            ref_cur = true;
+            ++refine_count;
+        }
+        if (stage != kFrozen) lg_cur += factor;
+        __syncwarp();
+        if (collect && accepted) {
+            round_trip_update(E, lower, upper, P.round_trip_margin, rt_state, trips);
+            warp_update_representatives(v, w, E, sp_s, lane);
+        }
+    }
+    // drain: no copy may land after the CTA exits
+    for (uint32_t s = 0; s < kSlots; ++s)
+        if (!wait_slot(s)) failed = true;
+    if (failed) {
+        if (lane == 0) record_error(ctl, WLG_ERR_TIMEOUT, w);
+        return;
+    }
+    if (lane == 0) {
+        lg_s[cur - wb] = lg_cur;
+        h_s[cur - wb] = hc_cur;
+        act_s[cur - wb] = act_cur ? 1 : 0;
+        if (nalivaiko) ref_s[cur - wb] = ref_cur ? 1 : 0;
+    }
+    __syncwarp();
+    for (int k = 0; k < kSlots; ++k) rng_step_back(rng);  // back over the queued, unconsumed draws
+
+    st.rng[0] = rng.s0;
+    st.rng[1] = rng.s1;
+    st.rng[2] = rng.s2;
+    st.rng[3] = rng.s3;
+    st.energy = E;
+    st.factor = factor;
+    st.stage = stage;
+    st.attempted = att0 + batch;
+    st.accepted += n_acc;
+    st.forced += n_forced;
+    st.last_accepted = st.attempted - since;
+    st.active_count = active_count;
+    st.refine_count = refine_count;
+    st.cur_bin = cur;
+    st.rt_state = rt_state;
+    st.round_trips = trips;
+
+    if (a.epoch_mode && st.stage == kWangLandau) {
+        const bool at_limit = P.max_attempts != 0 && st.attempted >= P.max_attempts;
+        if (st.attempted - st.last_check >= P.check_interval || at_limit) {
+            st.last_check = st.attempted;
+            const HistStats hs = warp_histogram_statistics(h_s, nalivaiko ? ref_s : act_s, nbins,
+                                                           nalivaiko ? st.refine_count : st.active_count, lane);
+            st.last_flatness = P.inverse_time ? hs.coverage : hs.min_over_mean;
+            if (stats_ready(hs, st.stage, P)) warp_begin_next_iteration(st, h_s, ref_s, nbins, P, lane);
+        }
+    }
+    {
+        const double2* src = reinterpret_cast<const double2*>(f);
+        double2* dst = reinterpret_cast<double2*>(fg);
+        for (int k = lane; k < (v.ld >> 1); k += 32) dst[k] = src[k];
+        const int4* ssrc = reinterpret_cast<const int4*>(sp_s);
+        int4* sdst = reinterpret_cast<int4*>(sg);
+        for (int k = lane; k < (v.ld >> 4); k += 32) sdst[k] = ssrc[k];
+    }
+    for (int b = lane; b < nbins; b += 32) {
+        v.log_g[boff + b] = lg_s[b];
+        v.hist[boff + b] = h_s[b];
+        v.active[boff + b] = act_s[b];
+        if constexpr (kFeat) {
+            v.refine[boff + b] = ref_s[b];
+            if (collect) {
+                v.sqdisp[boff + b] = sq_s[b];
+                v.dsamples[boff + b] = ds_s[b];
+            }
+        }
+    }
+    if (lane == 0) {
+        v.ws[w] = st;
+        if (a.epoch_mode) {
+            if (st.stage == kFrozen) atomicAdd(&ctl->frozen, 1u);
+            if (P.max_attempts != 0 && st.attempted >= P.max_attempts) atomicAdd(&ctl->at_limit, 1u);
+        }
+    }
+}
+
+using SweepFn = void (*)(EngineView, WalkArgs);
+
+template <int P, bool F>
+SweepFn sweep_fn() {
+    static bool configured = false;
+    if (!configured) {
+        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_dense_kernel<P, F>),
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+                   "cudaFuncSetAttribute");
+        configured = true;
+    }
+    return &sweep_dense_kernel<P, F>;
+}
+
+}  // namespace
+
+bool launch_sweep_dense(const EngineView& v, const WalkArgs& a, cudaStream_t stream) {
+    const bool features = v.p.collect || v.p.nalivaiko;
+    const size_t jbytes = v.precision == WLG_PRECISION_FP64 ? 8 : v.precision == WLG_PRECISION_FP32 ? 4 : 2;
+    const size_t bytes = ring_layout(v.ld, v.max_window_bins, features, jbytes).total;
+    if (bytes > 227 * 1024) return false;
+    SweepFn fn;
+    if (v.precision == WLG_PRECISION_FP32)
+        fn = features ? sweep_fn<WLG_PRECISION_FP32, true>() : sweep_fn<WLG_PRECISION_FP32, false>();
+    else if (v.precision == WLG_PRECISION_BF16)
+        fn = features ? sweep_fn<WLG_PRECISION_BF16, true>() : sweep_fn<WLG_PRECISION_BF16, false>();
+    else
+        fn = features ? sweep_fn<WLG_PRECISION_FP64, true>() : sweep_fn<WLG_PRECISION_FP64, false>();
+    fn<<<static_cast<unsigned>(a.count), 32, bytes, stream>>>(v, a);
+    check_cuda(cudaGetLastError(), "sweep_dense_kernel");
+    return true;
+}
+
+}  // namespace wlg

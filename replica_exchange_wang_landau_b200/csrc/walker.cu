@@ -138,27 +138,6 @@ __device__ __forceinline__ double warp_total_energy(const EngineView& v, const i
 
 // ---- shared-memory carve-up ---------------------------------------------------------------
 
-__host__ __device__ inline size_t round16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
-
-struct SmemLayout {
-    size_t fields, log_g, hist, sq, ds, spins, active, refine, total;
-};
-
-__host__ __device__ inline SmemLayout smem_layout(int ld, int mwb, bool smem_fields, bool features) {
-    SmemLayout L;
-    size_t at = 0;
-    L.fields = at; at += smem_fields ? static_cast<size_t>(ld) * 8 : 0;
-    L.log_g = at; at += round16(static_cast<size_t>(mwb) * 8);
-    L.hist = at; at += round16(static_cast<size_t>(mwb) * 8);
-    L.sq = at; at += features ? round16(static_cast<size_t>(mwb) * 8) : 0;
-    L.ds = at; at += features ? round16(static_cast<size_t>(mwb) * 8) : 0;
-    L.spins = at; at += round16(static_cast<size_t>(ld));
-    L.active = at; at += round16(static_cast<size_t>(mwb));
-    L.refine = at; at += features ? round16(static_cast<size_t>(mwb)) : 0;
-    L.total = at;
-    return L;
-}
-
 size_t walker_smem_bytes(const EngineView& v, bool smem_fields, bool features) {
     return smem_layout(v.ld, v.max_window_bins, smem_fields, features).total;
 }
@@ -401,421 +380,6 @@ __global__ void __launch_bounds__(256) walk_kernel(EngineView v, WalkArgs a) {
     }
 }
 
-// ---- the dense sweep with a TMA row ring -------------------------------------------------------
-//
-// The random site of every attempt is a draw of the walker's xoshiro stream, which does not
-// depend on the walk, so the draws are generated kRing ahead of their use and, for every
-// draw, the J row of the site it would select is fetched into a shared-memory ring slot by
-// a bulk asynchronous copy (cp.async.bulk, completion on an mbarrier).  When the draw is
-// consumed as a site and the flip is accepted, the row is already on chip; when it is
-// consumed as the acceptance uniform, its row is simply dropped.  The walker's own RNG
-// state advances one step per consumed draw, so the state written back is exactly the
-// reference's.  Every wait on an mbarrier is bounded; on timeout the walker records
-// WLG_ERR_TIMEOUT, drains its outstanding copies (bounded again) and stops.
-
-namespace ring {
-
-constexpr int kSlots = 8;
-constexpr uint32_t kWaitLimit = 1u << 18;  // polls; a row copy completes in about a microsecond
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Warp-uniform bounded wait for the phase `parity` of one slot's barrier.
-__device__ __forceinline__ bool wait(uint32_t bar, uint32_t parity) {
-    for (uint32_t k = 0; k < kWaitLimit; ++k)
-        if (__all_sync(kFull, mbar_try(bar, parity))) return true;
-    return false;
-}
-
-struct Layout {
-    size_t ring, bars, base, total;
-};
-__host__ __device__ inline Layout layout(int ld, int mwb, bool features, size_t jbytes) {
-    Layout L;
-    size_t at = 0;
-    L.ring = at;
-    at += kSlots * round16(static_cast<size_t>(ld) * jbytes);
-    L.bars = at;
-    at += round16(kSlots * 8);
-    L.base = at;
-    at += smem_layout(ld, mwb, true, features).total;
-    L.total = at;
-    return L;
-}
-
-}  // namespace ring
-
-template <int kPrec>
-struct CouplingType;
-template <> struct CouplingType<WLG_PRECISION_FP64> { using T = double; };
-template <> struct CouplingType<WLG_PRECISION_FP32> { using T = float; };
-template <> struct CouplingType<WLG_PRECISION_BF16> { using T = __nv_bfloat16; };
-
-// fields[j] += m * row[j] from a row held in shared memory
-template <int kPrec>
-__device__ __forceinline__ void ring_update(const void* row_smem, int ld, double m, double* f, int lane) {
-    double2* f2 = reinterpret_cast<double2*>(f);
-    if constexpr (kPrec == WLG_PRECISION_FP64) {
-        const double2* r = reinterpret_cast<const double2*>(row_smem);
-#pragma unroll 4
-        for (int k = lane; k < (ld >> 1); k += 32) {
-            const double2 a = r[k];
-            double2 h = f2[k];
-            h.x = fma(m, a.x, h.x);
-            h.y = fma(m, a.y, h.y);
-            f2[k] = h;
-        }
-    } else if constexpr (kPrec == WLG_PRECISION_FP32) {
-        const float4* r = reinterpret_cast<const float4*>(row_smem);
-#pragma unroll 2
-        for (int k = lane; k < (ld >> 2); k += 32) {
-            const float4 a = r[k];
-            double2 h0 = f2[2 * k], h1 = f2[2 * k + 1];
-            h0.x = fma(m, static_cast<double>(a.x), h0.x);
-            h0.y = fma(m, static_cast<double>(a.y), h0.y);
-            h1.x = fma(m, static_cast<double>(a.z), h1.x);
-            h1.y = fma(m, static_cast<double>(a.w), h1.y);
-            f2[2 * k] = h0;
-            f2[2 * k + 1] = h1;
-        }
-    } else {
-        const uint4* r = reinterpret_cast<const uint4*>(row_smem);
-        for (int k = lane; k < (ld >> 3); k += 32) {
-            const uint4 raw = r[k];
-            const uint32_t words[4] = {raw.x, raw.y, raw.z, raw.w};
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                double2 h = f2[4 * k + q];
-                h.x = fma(m, static_cast<double>(__uint_as_float(words[q] << 16)), h.x);
-                h.y = fma(m, static_cast<double>(__uint_as_float(words[q] & 0xffff0000u)), h.y);
-                f2[4 * k + q] = h;
-            }
-        }
-    }
-}
-
-template <int kPrec, bool kFeat>
-__global__ void __launch_bounds__(32, 1) walk_ring_kernel(EngineView v, WalkArgs a) {
-    using JT = typename CouplingType<kPrec>::T;
-    extern __shared__ __align__(128) unsigned char smem[];
-    const int lane = threadIdx.x & 31;
-    if (static_cast<int>(blockIdx.x) >= a.count) return;
-    const int w = a.first + static_cast<int>(blockIdx.x);
-    Control* ctl = v.ctl;
-    if (a.epoch_mode && *reinterpret_cast<volatile int32_t*>(&ctl->done)) return;
-
-    const ring::Layout RL = ring::layout(v.ld, v.max_window_bins, kFeat, sizeof(JT));
-    const SmemLayout L = smem_layout(v.ld, v.max_window_bins, true, kFeat);
-    unsigned char* base = smem + RL.base;
-    const JT* ring_rows = reinterpret_cast<const JT*>(smem + RL.ring);
-    double* f = reinterpret_cast<double*>(base + L.fields);
-    double* lg_s = reinterpret_cast<double*>(base + L.log_g);
-    uint64_t* h_s = reinterpret_cast<uint64_t*>(base + L.hist);
-    double* sq_s = reinterpret_cast<double*>(base + L.sq);
-    uint64_t* ds_s = reinterpret_cast<uint64_t*>(base + L.ds);
-    int8_t* sp_s = reinterpret_cast<int8_t*>(base + L.spins);
-    uint8_t* act_s = base + L.active;
-    uint8_t* ref_s = base + L.refine;
-
-    WalkerState st = v.ws[w];
-    const int wb = v.win_begin[st.window], we = v.win_end[st.window], nbins = we - wb;
-    const size_t boff = static_cast<size_t>(w) * static_cast<size_t>(v.grid.count) + static_cast<size_t>(wb);
-    double* fg = v.fields + static_cast<size_t>(st.slot) * v.ld;
-    int8_t* sg = v.spins + static_cast<size_t>(st.slot) * v.ld;
-    const DeviceParams& P = v.p;
-    const bool collect = kFeat && P.collect;
-    const bool nalivaiko = kFeat && P.nalivaiko;
-
-    const int cur0 = st.cur_bin;
-    if (cur0 < wb || cur0 >= we) {  // "Walker escaped its energy window"
-        if (lane == 0) record_error(ctl, WLG_ERR_ESCAPED, w);
-        return;
-    }
-    uint64_t batch;
-    if (a.fixed_batch) {
-        batch = a.fixed_batch;
-    } else {
-        batch = P.exchange_interval;
-        if (P.max_attempts) {
-            const uint64_t remaining = st.attempted < P.max_attempts ? P.max_attempts - st.attempted : 0;
-            batch = remaining < batch ? remaining : batch;
-        }
-    }
-
-    // ring set-up: barriers, then the first kSlots draws and their rows
-    const JT* J = kPrec == WLG_PRECISION_FP64 ? reinterpret_cast<const JT*>(v.J64)
-                  : kPrec == WLG_PRECISION_FP32 ? reinterpret_cast<const JT*>(v.J32)
-                                                : reinterpret_cast<const JT*>(v.J16);
-    const uint32_t row_bytes = static_cast<uint32_t>(v.ld * sizeof(JT));
-    const uint32_t ring_addr = ring::smem_addr(smem + RL.ring);
-    const uint32_t bar_addr = ring::smem_addr(smem + RL.bars);
-    if (lane == 0) {
-        for (int s = 0; s < ring::kSlots; ++s) ring::mbar_init(bar_addr + 8 * s);
-        ring::fence_mbar_init();
-    }
-    __syncwarp();
-    Rng crng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};  // consumed draws only
-    Rng prng = crng;                                       // kSlots draws ahead
-    uint64_t q[ring::kSlots];
-#pragma unroll
-    for (int k = 0; k < ring::kSlots; ++k) {
-        q[k] = prng.next();
-        if (lane == 0)
-            ring::bulk_load(ring_addr + k * row_bytes, J + fast_mod(v.site_mod, q[k]) * v.ld, row_bytes,
-                            bar_addr + 8 * k);
-    }
-    uint32_t parity = 0;                              // bit s: phase parity the next wait on slot s expects
-    uint32_t inflight = (1u << ring::kSlots) - 1u;   // bit s: a copy into slot s is not yet observed complete
-    bool failed = false;
-    auto wait_slot = [&](int s) {
-        if (!((inflight >> s) & 1u)) return true;
-        if (!ring::wait(bar_addr + 8 * s, (parity >> s) & 1u)) return false;
-        inflight &= ~(1u << s);
-        parity ^= 1u << s;
-        return true;
-    };
-
-    // stage the walker into shared memory (overlaps the first row copies)
-    {
-        const double2* src = reinterpret_cast<const double2*>(fg);
-        double2* dst = reinterpret_cast<double2*>(f);
-        for (int k = lane; k < (v.ld >> 1); k += 32) dst[k] = src[k];
-        const int4* ssrc = reinterpret_cast<const int4*>(sg);
-        int4* sdst = reinterpret_cast<int4*>(sp_s);
-        for (int k = lane; k < (v.ld >> 4); k += 32) sdst[k] = ssrc[k];
-    }
-    for (int b = lane; b < nbins; b += 32) {
-        lg_s[b] = v.log_g[boff + b];
-        h_s[b] = v.hist[boff + b];
-        act_s[b] = v.active[boff + b];
-        if constexpr (kFeat) {
-            ref_s[b] = v.refine[boff + b];
-            if (collect) {
-                sq_s[b] = v.sqdisp[boff + b];
-                ds_s[b] = v.dsamples[boff + b];
-            }
-        }
-    }
-    __syncwarp();
-    if (collect && st.rep_pending) {
-        warp_update_representatives(v, w, st.energy, sp_s, lane);
-        st.rep_pending = 0;
-    }
-
-    int head = 0;  // slot of q[0]
-    auto pop = [&]() {  // consume q[0]; its slot is refilled with the draw kSlots ahead
-        if (!wait_slot(head)) {
-            failed = true;
-            return;
-        }
-        (void)crng.next();
-#pragma unroll
-        for (int k = 0; k < ring::kSlots - 1; ++k) q[k] = q[k + 1];
-        q[ring::kSlots - 1] = prng.next();
-        __syncwarp();
-        if (lane == 0) {
-            ring::fence_proxy_async();
-            ring::bulk_load(ring_addr + head * row_bytes, J + fast_mod(v.site_mod, q[ring::kSlots - 1]) * v.ld,
-                            row_bytes, bar_addr + 8 * head);
-        }
-        inflight |= 1u << head;
-        head = (head + 1) & (ring::kSlots - 1);
-    };
-
-    double E = st.energy;
-    double factor = st.factor;
-    int32_t stage = st.stage;
-    uint64_t att = st.attempted, acc_n = st.accepted, forced_n = st.forced, last_acc = st.last_accepted;
-    uint64_t active_count = st.active_count, refine_count = st.refine_count;
-    int32_t rt_state = st.rt_state;
-    uint64_t trips = st.round_trips;
-    const double lower = window_lower(v, wb);
-    const double upper = window_lower(v, we);
-    int cur = cur0;
-    double lg_cur = lg_s[cur - wb];
-    uint64_t hc_cur = h_s[cur - wb];
-    bool act_cur = act_s[cur - wb] != 0;
-    bool ref_cur = nalivaiko ? ref_s[cur - wb] != 0 : true;
-    const uint64_t threshold = v.site_mod.threshold;
-
-    for (uint64_t t = 0; t < batch && !failed;) {
-        const uint64_t x = q[0];
-        if (x < threshold) {  // bounded() rejected this draw; the next one is the site
-            pop();
-            continue;
-        }
-        const int i = static_cast<int>(fast_mod(v.site_mod, x));
-        const int slot = head;
-        const int8_t si = sp_s[i];
-        const double delta = -2.0 * static_cast<double>(si) * f[i];
-        const double Ep = E + delta;
-        const int64_t nb = grid_index(v.grid, Ep);
-        bool accepted = false, forced = false, used_uniform = false;
-        double lg_new = 0.0;
-        if (nb >= wb && nb < we) {
-            lg_new = nb == cur ? lg_cur : lg_s[nb - wb];
-            const double log_ratio = lg_cur - lg_new;
-            const bool force_due = P.force_after != 0 && att - last_acc >= P.force_after;
-            if (log_ratio >= 0.0) {
-                accepted = true;
-            } else if (force_due) {
-                accepted = forced = true;
-            } else {
-                used_uniform = true;
-                accepted = log_uniform_below(to_uniform(q[1]), log_ratio);
-            }
-        }
-        ++att;
-        if (accepted) {
-            double m = -2.0 * static_cast<double>(si);
-            if constexpr (kPrec == WLG_PRECISION_BF16) m *= static_cast<double>(__ldg(v.Jscale + i));
-            if (!wait_slot(slot)) {
-                failed = true;
-                break;
-            }
-            ring_update<kPrec>(ring_rows + static_cast<size_t>(slot) * v.ld, v.ld, m, f, lane);
-            if (lane == 0) sp_s[i] = static_cast<int8_t>(-si);
-            E = Ep;
-            ++acc_n;
-            if (forced) ++forced_n;
-            last_acc = att;
-        }
-        pop();                   // the site draw: its slot is free once the update has read it
-        if (used_uniform) pop(); // the acceptance uniform
-        if (collect && lane == 0) {
-            const double displacement = accepted ? delta : 0.0;
-            sq_s[cur - wb] += displacement * displacement;
-            ++ds_s[cur - wb];
-        }
-        if (stage == kInverseTime) {
-            if (active_count != 0 && att != 0)
-                factor = static_cast<double>(active_count) / static_cast<double>(att);
-            if (factor <= P.final_factor) stage = kFrozen;
-        }
-        if (accepted && nb != cur) {
-            if (lane == 0) {
-                lg_s[cur - wb] = lg_cur;
-                h_s[cur - wb] = hc_cur;
-                act_s[cur - wb] = act_cur ? 1 : 0;
-                if (nalivaiko) ref_s[cur - wb] = ref_cur ? 1 : 0;
-            }
-            cur = static_cast<int>(nb);
-            lg_cur = lg_new;
-            hc_cur = h_s[cur - wb];
-            act_cur = act_s[cur - wb] != 0;
-            ref_cur = nalivaiko ? ref_s[cur - wb] != 0 : true;
-        }
-        ++hc_cur;
-        if (!act_cur) {
-            act_cur = true;
-            ++active_count;
-        }
-        if (nalivaiko && !ref_cur) {
-            ref_cur = true;
-            ++refine_count;
-        }
-        if (stage != kFrozen) lg_cur += factor;
-        __syncwarp();
-        if (collect && accepted) {
-            round_trip_update(E, lower, upper, P.round_trip_margin, rt_state, trips);
-            warp_update_representatives(v, w, E, sp_s, lane);
-        }
-        ++t;
-    }
-    // drain: no copy may land after the CTA has exited
-    for (int s = 0; s < ring::kSlots; ++s)
-        if (!wait_slot(s)) failed = true;
-    if (failed) {
-        if (lane == 0) record_error(ctl, WLG_ERR_TIMEOUT, w);
-        return;
-    }
-    if (lane == 0) {
-        lg_s[cur - wb] = lg_cur;
-        h_s[cur - wb] = hc_cur;
-        act_s[cur - wb] = act_cur ? 1 : 0;
-        if (nalivaiko) ref_s[cur - wb] = ref_cur ? 1 : 0;
-    }
-    __syncwarp();
-
-    st.rng[0] = crng.s0; st.rng[1] = crng.s1; st.rng[2] = crng.s2; st.rng[3] = crng.s3;
-    st.energy = E;
-    st.factor = factor;
-    st.stage = stage;
-    st.attempted = att;
-    st.accepted = acc_n;
-    st.forced = forced_n;
-    st.last_accepted = last_acc;
-    st.active_count = active_count;
-    st.refine_count = refine_count;
-    st.cur_bin = cur;
-    st.rt_state = rt_state;
-    st.round_trips = trips;
-
-    if (a.epoch_mode && st.stage == kWangLandau) {
-        const bool at_limit = P.max_attempts != 0 && st.attempted >= P.max_attempts;
-        if (st.attempted - st.last_check >= P.check_interval || at_limit) {
-            st.last_check = st.attempted;
-            const HistStats hs = warp_histogram_statistics(h_s, nalivaiko ? ref_s : act_s, nbins,
-                                                           nalivaiko ? st.refine_count : st.active_count, lane);
-            st.last_flatness = P.inverse_time ? hs.coverage : hs.min_over_mean;
-            if (stats_ready(hs, st.stage, P)) warp_begin_next_iteration(st, h_s, ref_s, nbins, P, lane);
-        }
-    }
-    {
-        const double2* src = reinterpret_cast<const double2*>(f);
-        double2* dst = reinterpret_cast<double2*>(fg);
-        for (int k = lane; k < (v.ld >> 1); k += 32) dst[k] = src[k];
-        const int4* ssrc = reinterpret_cast<const int4*>(sp_s);
-        int4* sdst = reinterpret_cast<int4*>(sg);
-        for (int k = lane; k < (v.ld >> 4); k += 32) sdst[k] = ssrc[k];
-    }
-    for (int b = lane; b < nbins; b += 32) {
-        v.log_g[boff + b] = lg_s[b];
-        v.hist[boff + b] = h_s[b];
-        v.active[boff + b] = act_s[b];
-        if constexpr (kFeat) {
-            v.refine[boff + b] = ref_s[b];
-            if (collect) {
-                v.sqdisp[boff + b] = sq_s[b];
-                v.dsamples[boff + b] = ds_s[b];
-            }
-        }
-    }
-    if (lane == 0) {
-        v.ws[w] = st;
-        if (a.epoch_mode) {
-            if (st.stage == kFrozen) atomicAdd(&ctl->frozen, 1u);
-            if (P.max_attempts != 0 && st.attempted >= P.max_attempts) atomicAdd(&ctl->at_limit, 1u);
-        }
-    }
-}
-
-size_t ring_smem_bytes(const EngineView& v, bool features) {
-    const size_t jbytes = v.precision == WLG_PRECISION_FP64 ? 8 : v.precision == WLG_PRECISION_FP32 ? 4 : 2;
-    return ring::layout(v.ld, v.max_window_bins, features, jbytes).total;
-}
-
 // ---- initialisation: the WangLandauWalker constructor --------------------------------------
 
 template <int kPrec, bool kCsr, bool kSmemF, bool kFeat>
@@ -1023,29 +587,9 @@ static InitFn pick_init(bool csr, bool smem_fields, bool features) {
 
 static bool features_of(const EngineView& v) { return v.p.collect || v.p.nalivaiko; }
 
-template <int P, bool F>
-static WalkFn ring_fn() {
-    set_smem_attr<P + 16, false, true, F>(reinterpret_cast<const void*>(&walk_ring_kernel<P, F>));
-    return &walk_ring_kernel<P, F>;
-}
-
-static WalkFn pick_ring(int precision, bool features) {
-    if (precision == WLG_PRECISION_FP32) return features ? ring_fn<WLG_PRECISION_FP32, true>() : ring_fn<WLG_PRECISION_FP32, false>();
-    if (precision == WLG_PRECISION_BF16) return features ? ring_fn<WLG_PRECISION_BF16, true>() : ring_fn<WLG_PRECISION_BF16, false>();
-    return features ? ring_fn<WLG_PRECISION_FP64, true>() : ring_fn<WLG_PRECISION_FP64, false>();
-}
-
 void launch_walk(const EngineView& v, const WalkArgs& a, int wpb, cudaStream_t stream) {
     const bool features = features_of(v);
-    if (!v.csr) {  // dense couplings: the TMA row ring, one walker per CTA
-        const size_t bytes = ring_smem_bytes(v, features);
-        if (bytes <= 227 * 1024) {
-            WalkFn fn = pick_ring(v.precision, features);
-            fn<<<static_cast<unsigned>(a.count), 32, bytes, stream>>>(v, a);
-            check_cuda(cudaGetLastError(), "walk_ring_kernel");
-            return;
-        }
-    }
+    if (!v.csr && launch_sweep_dense(v, a, stream)) return;  // sweep.cu: the TMA row ring
     const bool smem_fields = a.smem_per_walker >= static_cast<int>(walker_smem_bytes(v, true, features));
     WalkFn fn = pick_walk(v.precision, v.csr != 0, smem_fields, features);
     wpb = std::max(1, std::min(wpb, 8));

@@ -156,6 +156,29 @@ __device__ __forceinline__ void warp_update_representatives(const EngineView& v,
     }
 }
 
+// ---- shared-memory carve-up of one walker --------------------------------------------
+
+__host__ __device__ inline size_t round16(size_t x) { return (x + 15) & ~static_cast<size_t>(15); }
+
+struct SmemLayout {
+    size_t fields, log_g, hist, sq, ds, spins, active, refine, total;
+};
+
+__host__ __device__ inline SmemLayout smem_layout(int ld, int mwb, bool smem_fields, bool features) {
+    SmemLayout L;
+    size_t at = 0;
+    L.fields = at; at += smem_fields ? static_cast<size_t>(ld) * 8 : 0;
+    L.log_g = at; at += round16(static_cast<size_t>(mwb) * 8);
+    L.hist = at; at += round16(static_cast<size_t>(mwb) * 8);
+    L.sq = at; at += features ? round16(static_cast<size_t>(mwb) * 8) : 0;
+    L.ds = at; at += features ? round16(static_cast<size_t>(mwb) * 8) : 0;
+    L.spins = at; at += round16(static_cast<size_t>(ld));
+    L.active = at; at += round16(static_cast<size_t>(mwb));
+    L.refine = at; at += features ? round16(static_cast<size_t>(mwb)) : 0;
+    L.total = at;
+    return L;
+}
+
 __device__ __forceinline__ double window_lower(const EngineView& v, int wb) {
     return v.grid.minimum + static_cast<double>(wb) * v.grid.width;
 }

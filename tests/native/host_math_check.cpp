@@ -48,6 +48,20 @@ int main() {
             return 1;
         }
     }
+    // rng_step_back inverts Rng::next() exactly
+    for (int k = 0; k < 100000; ++k) {
+        wlg::Rng a;
+        a.seed(rng.next(), rng.next());
+        const int steps = 1 + k % 9;
+        wlg::Rng b = a;
+        for (int s = 0; s < steps; ++s) (void)b.next();
+        for (int s = 0; s < steps; ++s) wlg::rng_step_back(b);
+        if (a.s0 != b.s0 || a.s1 != b.s1 || a.s2 != b.s2 || a.s3 != b.s3) {
+            std::printf("rng_step_back mismatch at case %d\n", k);
+            return 1;
+        }
+        ++cases;
+    }
     std::printf("ok %" PRIu64 "\n", cases);
     return 0;
 }
