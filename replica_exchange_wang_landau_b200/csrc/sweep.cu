@@ -443,6 +443,324 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_kernel(EngineView v, WalkAr
     }
 }
 
+// ---- the lookahead sweep (no pilot statistics, no Nalivaiko mask) ------------------------
+//
+// The same attempt as above, reorganised so that the N-element field update is not on the
+// path from one attempt to the next.  The next attempt's site is the draw after the site
+// draw (q1) or, when this attempt consumes the acceptance uniform, the one after that (q2).
+// Before deciding, the warp loads for both candidates their field, spin and the J entry of
+// the current site's row (which is resident in the ring); after deciding it forms the next
+// attempt's field with one fma.  The full update of all N fields then runs off the chain with
+// m_eff = accepted ? m : 0: adding m*0 changes no field, because a field is never -0.0 (the
+// sums start at +0.0, and a sum that reaches zero is +0.0), so the fields stay bit-identical
+// to the reference's.  Every branch in the loop is rare (a rejected bounded() draw, an
+// acceptance test inside the log margin, a first visit, a slow copy), so the compiler can
+// interleave the independent work (ring refills, RNG, the update) with the chain.
+
+constexpr int kFastSlots = 8;
+
+template <class JT> __device__ __forceinline__ double jval(JT x) { return static_cast<double>(x); }
+template <> __device__ __forceinline__ double jval<__nv_bfloat16>(__nv_bfloat16 x) {
+    return static_cast<double>(__bfloat162float(x));
+}
+
+// Single-lane issue of one or (when `second`) two row copies into slots s0 and s1.
+__device__ __forceinline__ void issue_rows(uint32_t dst0, const void* src0, uint32_t bar0, uint32_t dst1,
+                                           const void* src1, uint32_t bar1, uint32_t bytes, bool second) {
+    const uint32_t two = second ? 1u : 0u;
+    asm volatile(
+        "{\n .reg .pred p, q;\n elect.sync _|p, 0xffffffff;\n"
+        " setp.ne.u32 q, %7, 0;\n"
+        " and.pred q, q, p;\n"
+        " @p fence.proxy.async.shared::cta;\n"
+        " @p mbarrier.arrive.expect_tx.shared::cta.b64 _, [%2], %6;\n"
+        " @p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %6, [%2];\n"
+        " @q mbarrier.arrive.expect_tx.shared::cta.b64 _, [%5], %6;\n"
+        " @q cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%3], [%4], %6, [%5];\n}" ::"r"(dst0),
+        "l"(src0), "r"(bar0), "r"(dst1), "l"(src1), "r"(bar1), "r"(bytes), "r"(two)
+        : "memory");
+}
+
+template <int kPrec>
+__global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, WalkArgs a) {
+    using JT = typename CouplingType<kPrec>::T;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    if (static_cast<int>(blockIdx.x) >= a.count) return;
+    const int w = a.first + static_cast<int>(blockIdx.x);
+    Control* ctl = v.ctl;
+    if (a.epoch_mode && *reinterpret_cast<volatile int32_t*>(&ctl->done)) return;
+
+    // carve-up: [ring of kFastSlots rows][barriers][fields, log_g, H, spins, active]
+    const size_t row_stride = round16(static_cast<size_t>(v.ld) * sizeof(JT));
+    const size_t bars_at = kFastSlots * row_stride;
+    const size_t base_at = bars_at + round16(kFastSlots * 8);
+    const SmemLayout L = smem_layout(v.ld, v.max_window_bins, true, false);
+    unsigned char* base = smem + base_at;
+    const JT* ring_rows = reinterpret_cast<const JT*>(smem);
+    double* f = reinterpret_cast<double*>(base + L.fields);
+    double* lg_s = reinterpret_cast<double*>(base + L.log_g);
+    uint64_t* h_s = reinterpret_cast<uint64_t*>(base + L.hist);
+    int8_t* sp_s = reinterpret_cast<int8_t*>(base + L.spins);
+    uint8_t* act_s = base + L.active;
+
+    WalkerState st = v.ws[w];
+    const int wb = v.win_begin[st.window], we = v.win_end[st.window], nbins = we - wb;
+    const size_t boff = static_cast<size_t>(w) * static_cast<size_t>(v.grid.count) + static_cast<size_t>(wb);
+    double* fg = v.fields + static_cast<size_t>(st.slot) * v.ld;
+    int8_t* sg = v.spins + static_cast<size_t>(st.slot) * v.ld;
+    const DeviceParams& P = v.p;
+    if (st.cur_bin < wb || st.cur_bin >= we) {  // "Walker escaped its energy window"
+        if (lane == 0) record_error(ctl, WLG_ERR_ESCAPED, w);
+        return;
+    }
+    uint32_t batch;
+    {
+        uint64_t b = a.fixed_batch ? a.fixed_batch : P.exchange_interval;
+        if (!a.fixed_batch && P.max_attempts) {
+            const uint64_t remaining = st.attempted < P.max_attempts ? P.max_attempts - st.attempted : 0;
+            b = remaining < b ? remaining : b;
+        }
+        batch = static_cast<uint32_t>(b < 0xffffffffULL ? b : 0xffffffffULL);
+    }
+
+    const JT* J = kPrec == WLG_PRECISION_FP64   ? reinterpret_cast<const JT*>(v.J64)
+                  : kPrec == WLG_PRECISION_FP32 ? reinterpret_cast<const JT*>(v.J32)
+                                                : reinterpret_cast<const JT*>(v.J16);
+    const uint32_t row_bytes = static_cast<uint32_t>(v.ld * sizeof(JT));
+    const uint32_t rs = static_cast<uint32_t>(row_stride);
+    const uint32_t ring_addr = smem_addr(smem);
+    const uint32_t bar_addr = smem_addr(smem + bars_at);
+    if (lane == 0) {
+        for (int s = 0; s < kFastSlots; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_addr + 8 * s) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    const FastMod fm = v.site_mod;
+    Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};
+    uint64_t q0 = rng.next(), q1 = rng.next(), q2 = rng.next(), q3 = rng.next();
+    uint64_t q4 = rng.next(), q5 = rng.next(), q6 = rng.next(), q7 = rng.next();
+    {
+        const uint64_t qs[kFastSlots] = {q0, q1, q2, q3, q4, q5, q6, q7};
+#pragma unroll
+        for (int s = 0; s < kFastSlots; ++s)
+            issue_row(ring_addr + s * rs, J + fast_mod(fm, qs[s]) * v.ld, row_bytes, bar_addr + 8 * s, false);
+    }
+    uint32_t parity = 0;  // bit s: the phase parity the next wait on slot s expects
+    uint32_t head = 0;    // slot of q0
+    bool failed = false;
+    // Every slot has exactly one copy in flight except between its wait and its refill.
+    auto wait_slot = [&](uint32_t s) -> bool {
+        const uint32_t bar = bar_addr + 8 * s, par = (parity >> s) & 1u;
+        if (!__all_sync(kFull, mbar_try(bar, par)))
+            if (!mbar_wait(bar, par)) return false;
+        parity ^= 1u << s;
+        return true;
+    };
+
+    // stage the walker (overlaps the first copies)
+    {
+        const double2* src = reinterpret_cast<const double2*>(fg);
+        double2* dst = reinterpret_cast<double2*>(f);
+        for (int k = lane; k < (v.ld >> 1); k += 32) dst[k] = src[k];
+        const int4* ssrc = reinterpret_cast<const int4*>(sg);
+        int4* sdst = reinterpret_cast<int4*>(sp_s);
+        for (int k = lane; k < (v.ld >> 4); k += 32) sdst[k] = ssrc[k];
+    }
+    for (int b = lane; b < nbins; b += 32) {
+        lg_s[b] = v.log_g[boff + b];
+        h_s[b] = v.hist[boff + b];
+        act_s[b] = v.active[boff + b];
+    }
+    __syncwarp();
+
+    double E = st.energy;
+    double factor = st.factor;
+    int32_t stage = st.stage;
+    const uint64_t att0 = st.attempted;
+    uint64_t since = st.attempted - st.last_accepted;
+    uint32_t n_acc = 0, n_forced = 0;
+    uint64_t active_count = st.active_count;
+    const Grid g = v.grid;
+    const int gcount = static_cast<int>(g.count);
+    int cur = st.cur_bin;
+    double lg_cur = lg_s[cur - wb];
+    const uint64_t threshold = fm.threshold;
+    double factor_next = factor;
+    if (stage == kInverseTime && active_count != 0)
+        factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + 1);
+
+    int i = static_cast<int>(fast_mod(fm, q0));
+    int si = sp_s[i];
+    double h = f[i];
+
+    for (uint32_t t = 0; t < batch;) {
+        if (q0 < threshold) {  // rare: bounded() rejects this draw, the next one is the site
+            if (!wait_slot(head)) { failed = true; break; }
+            q0 = q1; q1 = q2; q2 = q3; q3 = q4; q4 = q5; q5 = q6; q6 = q7; q7 = rng.next();
+            issue_row(ring_addr + head * rs, J + fast_mod(fm, q7) * v.ld, row_bytes, bar_addr + 8 * head, false);
+            head = (head + 1) & (kFastSlots - 1);
+            __syncwarp();
+            i = static_cast<int>(fast_mod(fm, q0));
+            si = sp_s[i];
+            h = f[i];
+            continue;
+        }
+        if (!wait_slot(head)) { failed = true; break; }  // the current site's row is resident
+        const JT* row = ring_rows + static_cast<size_t>(head) * (row_stride / sizeof(JT));
+        // lookahead: the two candidates for the next site
+        const int c1 = static_cast<int>(fast_mod(fm, q1)), c2 = static_cast<int>(fast_mod(fm, q2));
+        const double f1 = f[c1], f2 = f[c2];
+        const int s1 = sp_s[c1], s2 = sp_s[c2];
+        const double r1 = jval(row[c1]), r2 = jval(row[c2]);
+        const double up = fmax(to_uniform(q1), 0x1.0p-53);
+        const double est = static_cast<double>(__log2f(static_cast<float>(up))) * 0.6931471805599453;
+        double scale = 1.0;
+        if constexpr (kPrec == WLG_PRECISION_BF16) scale = static_cast<double>(__ldg(v.Jscale + i));
+
+        // the decision (attempt_flip, src/wang_landau.cpp:244-262)
+        const double m = si > 0 ? -2.0 : 2.0;  // -2 * spin
+        const double delta = m * h;
+        const double Ep = E + delta;
+        const double off = Ep - g.minimum;
+        const double qv = g.pow2_width ? off * g.inv_width : off / g.width;
+        int nb = (Ep >= g.minimum && Ep <= g.maximum) ? __double2int_rd(qv) : -1;
+        nb = (nb == gcount && Ep == g.maximum) ? gcount - 1 : nb;
+        const bool in_window = nb >= wb && nb < we;
+        const double lg_load = lg_s[in_window ? nb - wb : 0];
+        const double lg_new = nb == cur ? lg_cur : lg_load;
+        const double log_ratio = lg_cur - lg_new;
+        const bool det = log_ratio >= 0.0;
+        const bool forced = !det && P.force_after != 0 && since >= P.force_after;
+        const bool need_u = in_window && !det && !forced;
+        bool u_ok = est < log_ratio - 1e-3;
+        if (need_u && !u_ok && !(est > log_ratio + 1e-3)) u_ok = log(up) < log_ratio;  // inside the margin
+        const bool accepted = in_window && (det || forced || u_ok);
+
+        // the next attempt's site, field and spin
+        const int c = need_u ? c2 : c1;
+        const double m_eff = (accepted ? m : 0.0) * scale;
+        const double h_next = fma(m_eff, need_u ? r2 : r1, need_u ? f2 : f1);
+        const int s_next = (accepted && c == i) ? -si : (need_u ? s2 : s1);
+
+        // add_flip_delta, off the chain (m_eff = 0 leaves every field unchanged)
+        row_update<kPrec>(row, v.ld, m_eff, f, lane);
+        if (lane == 0 && accepted) sp_s[i] = static_cast<int8_t>(-si);
+        E = accepted ? Ep : E;
+        since = accepted ? 0 : since + 1;
+        n_acc += accepted ? 1u : 0u;
+        n_forced += (accepted && forced) ? 1u : 0u;
+        ++t;
+
+        // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
+        if (stage == kInverseTime) {
+            factor = factor_next;
+            if (factor <= P.final_factor) stage = kFrozen;
+        }
+        const bool move = accepted && nb != cur;
+        if (lane == 0) lg_s[cur - wb] = lg_cur;
+        const int ncur = move ? nb : cur;
+        const double lg_base = move ? lg_new : lg_cur;
+        const uint64_t hv = h_s[ncur - wb];
+        const bool visited = act_s[ncur - wb] != 0;
+        if (lane == 0) h_s[ncur - wb] = hv + 1;
+        if (!visited) {  // rare: first visit of a bin
+            if (lane == 0) act_s[ncur - wb] = 1;
+            ++active_count;
+        }
+        cur = ncur;
+        lg_cur = stage != kFrozen ? lg_base + factor : lg_base;
+        if (stage == kInverseTime && active_count != 0)
+            factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + t + 1);
+
+        // ring: the site draw (and the uniform, when used) leave; their slots get new draws
+        const uint32_t sA = head, sB = (head + 1) & (kFastSlots - 1);
+        if (need_u) {
+            if (!wait_slot(sB)) { failed = true; break; }
+        }
+        const uint64_t d1 = rng.next();
+        Rng r2n = rng;
+        const uint64_t d2 = r2n.next();
+        if (need_u) rng = r2n;
+        __syncwarp();  // all lanes' reads of the site's row precede its refill
+        // d1 lands in the site's slot; d2 (only when the uniform was used) in the uniform's
+        issue_rows(ring_addr + sA * rs, J + fast_mod(fm, d1) * v.ld, bar_addr + 8 * sA, ring_addr + sB * rs,
+                   J + fast_mod(fm, d2) * v.ld, bar_addr + 8 * sB, row_bytes, need_u);
+        q0 = need_u ? q2 : q1;
+        q1 = need_u ? q3 : q2;
+        q2 = need_u ? q4 : q3;
+        q3 = need_u ? q5 : q4;
+        q4 = need_u ? q6 : q5;
+        q5 = need_u ? q7 : q6;
+        q6 = need_u ? d1 : q7;
+        q7 = need_u ? d2 : d1;
+        head = (head + (need_u ? 2u : 1u)) & (kFastSlots - 1);
+        i = c;
+        si = s_next;
+        h = h_next;
+        __syncwarp();
+    }
+    for (uint32_t s = 0; s < kFastSlots; ++s)  // drain: no copy may land after the CTA exits
+        if (!wait_slot(s)) failed = true;
+    if (failed) {
+        if (lane == 0) record_error(ctl, WLG_ERR_TIMEOUT, w);
+        return;
+    }
+    if (lane == 0) lg_s[cur - wb] = lg_cur;
+    __syncwarp();
+    for (int k = 0; k < kFastSlots; ++k) rng_step_back(rng);  // back over the queued draws
+
+    st.rng[0] = rng.s0;
+    st.rng[1] = rng.s1;
+    st.rng[2] = rng.s2;
+    st.rng[3] = rng.s3;
+    st.energy = E;
+    st.factor = factor;
+    st.stage = stage;
+    st.attempted = att0 + batch;
+    st.accepted += n_acc;
+    st.forced += n_forced;
+    st.last_accepted = st.attempted - since;
+    st.active_count = active_count;
+    st.cur_bin = cur;
+
+    if (a.epoch_mode && st.stage == kWangLandau) {
+        const bool at_limit = P.max_attempts != 0 && st.attempted >= P.max_attempts;
+        if (st.attempted - st.last_check >= P.check_interval || at_limit) {
+            st.last_check = st.attempted;
+            const HistStats hs = warp_histogram_statistics(h_s, act_s, nbins, st.active_count, lane);
+            st.last_flatness = P.inverse_time ? hs.coverage : hs.min_over_mean;
+            if (stats_ready(hs, st.stage, P)) warp_begin_next_iteration(st, h_s, nullptr, nbins, P, lane);
+        }
+    }
+    {
+        const double2* src = reinterpret_cast<const double2*>(f);
+        double2* dst = reinterpret_cast<double2*>(fg);
+        for (int k = lane; k < (v.ld >> 1); k += 32) dst[k] = src[k];
+        const int4* ssrc = reinterpret_cast<const int4*>(sp_s);
+        int4* sdst = reinterpret_cast<int4*>(sg);
+        for (int k = lane; k < (v.ld >> 4); k += 32) sdst[k] = ssrc[k];
+    }
+    for (int b = lane; b < nbins; b += 32) {
+        v.log_g[boff + b] = lg_s[b];
+        v.hist[boff + b] = h_s[b];
+        v.active[boff + b] = act_s[b];
+    }
+    if (lane == 0) {
+        v.ws[w] = st;
+        if (a.epoch_mode) {
+            if (st.stage == kFrozen) atomicAdd(&ctl->frozen, 1u);
+            if (P.max_attempts != 0 && st.attempted >= P.max_attempts) atomicAdd(&ctl->at_limit, 1u);
+        }
+    }
+}
+
+size_t fast_smem_bytes(const EngineView& v, size_t jbytes) {
+    return kFastSlots * round16(static_cast<size_t>(v.ld) * jbytes) + round16(kFastSlots * 8) +
+           smem_layout(v.ld, v.max_window_bins, true, false).total;
+}
+
 using SweepFn = void (*)(EngineView, WalkArgs);
 
 template <int P, bool F>
@@ -459,9 +777,32 @@ SweepFn sweep_fn() {
 
 }  // namespace
 
+template <int P>
+SweepFn fast_fn() {
+    static bool configured = false;
+    if (!configured) {
+        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_dense_fast_kernel<P>),
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+                   "cudaFuncSetAttribute");
+        configured = true;
+    }
+    return &sweep_dense_fast_kernel<P>;
+}
+
 bool launch_sweep_dense(const EngineView& v, const WalkArgs& a, cudaStream_t stream) {
     const bool features = v.p.collect || v.p.nalivaiko;
     const size_t jbytes = v.precision == WLG_PRECISION_FP64 ? 8 : v.precision == WLG_PRECISION_FP32 ? 4 : 2;
+    if (!features) {  // the lookahead sweep
+        const size_t fast_bytes = fast_smem_bytes(v, jbytes);
+        if (fast_bytes <= 227 * 1024) {
+            SweepFn fn = v.precision == WLG_PRECISION_FP32   ? fast_fn<WLG_PRECISION_FP32>()
+                         : v.precision == WLG_PRECISION_BF16 ? fast_fn<WLG_PRECISION_BF16>()
+                                                             : fast_fn<WLG_PRECISION_FP64>();
+            fn<<<static_cast<unsigned>(a.count), 32, fast_bytes, stream>>>(v, a);
+            check_cuda(cudaGetLastError(), "sweep_dense_fast_kernel");
+            return true;
+        }
+    }
     const size_t bytes = ring_layout(v.ld, v.max_window_bins, features, jbytes).total;
     if (bytes > 227 * 1024) return false;
     SweepFn fn;
