@@ -443,47 +443,46 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_kernel(EngineView v, WalkAr
     }
 }
 
-// ---- the lookahead sweep (no pilot statistics, no Nalivaiko mask) ------------------------
+// ---- the lookahead sweep (FP64 couplings, no pilot statistics, no Nalivaiko mask) --------
 //
 // The same attempt as above, reorganised so that the N-element field update is not on the
-// path from one attempt to the next.  The next attempt's site is the draw after the site
-// draw (q1) or, when this attempt consumes the acceptance uniform, the one after that (q2).
-// Before deciding, the warp loads for both candidates their field, spin and the J entry of
-// the current site's row (which is resident in the ring); after deciding it forms the next
-// attempt's field with one fma.  The full update of all N fields then runs off the chain with
-// m_eff = accepted ? m : 0: adding m*0 changes no field, because a field is never -0.0 (the
-// sums start at +0.0, and a sum that reaches zero is +0.0), so the fields stay bit-identical
-// to the reference's.  Every branch in the loop is rare (a rejected bounded() draw, an
-// acceptance test inside the log margin, a first visit, a slow copy), so the compiler can
-// interleave the independent work (ring refills, RNG, the update) with the chain.
+// path from one attempt to the next, and so that the loop body is one branch-free block the
+// compiler can schedule freely:
+//
+// * The next attempt's site is the draw after the site draw (q1) or, when this attempt
+//   consumes the acceptance uniform, the one after that (q2).  Before deciding, the warp
+//   loads for both candidates their field, spin and the J entry of the current site's row;
+//   after deciding it forms the next attempt's field with one fma.
+// * The update of all N fields then runs off the chain with m_eff = accepted ? m : 0: adding
+//   m*0 changes no field, because a field is never -0.0 (sums start at +0.0 and a sum that
+//   reaches zero is +0.0), so the fields stay bit-identical to the reference's.  Each lane
+//   keeps its share of the fields in registers and writes them through to shared memory,
+//   where the random single-field reads find them.
+// * Rows arrive by per-lane cp.async copies, one commit group per attempt: each lane copies
+//   exactly the 16-byte chunks of the row it will update.  A draw appended to the queue
+//   reaches its head no earlier than four attempts later (it enters at position >= 6 and
+//   moves by at most 2 per attempt), so "all but the 3 newest groups complete" covers the
+//   site's row and "all but the 2 newest" the next draw's slot before it is reused; both
+//   waits are single instructions.  When the uniform is not consumed, the second copy of the
+//   attempt is a zero-size copy into a spare slot, so every attempt commits exactly one group.
+// * The draws live in a small shared-memory queue; the generator runs kQueue draws ahead and
+//   is stepped back over them at the end of the batch.
+// Rare events (a rejected bounded() draw, an acceptance test inside the log margin, a first
+// visit of a bin) take branches.
 
-constexpr int kFastSlots = 8;
+constexpr int kQueue = 8;       // draws generated ahead; row slots in the ring
+constexpr int kQueueMask = 15;  // shared-memory draw queue of 16 entries
 
-template <class JT> __device__ __forceinline__ double jval(JT x) { return static_cast<double>(x); }
-template <> __device__ __forceinline__ double jval<__nv_bfloat16>(__nv_bfloat16 x) {
-    return static_cast<double>(__bfloat162float(x));
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int kPending> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(kPending) : "memory");
 }
 
-// Single-lane issue of one or (when `second`) two row copies into slots s0 and s1.
-__device__ __forceinline__ void issue_rows(uint32_t dst0, const void* src0, uint32_t bar0, uint32_t dst1,
-                                           const void* src1, uint32_t bar1, uint32_t bytes, bool second) {
-    const uint32_t two = second ? 1u : 0u;
-    asm volatile(
-        "{\n .reg .pred p, q;\n elect.sync _|p, 0xffffffff;\n"
-        " setp.ne.u32 q, %7, 0;\n"
-        " and.pred q, q, p;\n"
-        " @p fence.proxy.async.shared::cta;\n"
-        " @p mbarrier.arrive.expect_tx.shared::cta.b64 _, [%2], %6;\n"
-        " @p cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %6, [%2];\n"
-        " @q mbarrier.arrive.expect_tx.shared::cta.b64 _, [%5], %6;\n"
-        " @q cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%3], [%4], %6, [%5];\n}" ::"r"(dst0),
-        "l"(src0), "r"(bar0), "r"(dst1), "l"(src1), "r"(bar1), "r"(bytes), "r"(two)
-        : "memory");
-}
-
-template <int kPrec>
+template <int kChunks>
 __global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, WalkArgs a) {
-    using JT = typename CouplingType<kPrec>::T;
     extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     if (static_cast<int>(blockIdx.x) >= a.count) return;
@@ -491,14 +490,14 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, W
     Control* ctl = v.ctl;
     if (a.epoch_mode && *reinterpret_cast<volatile int32_t*>(&ctl->done)) return;
 
-    // carve-up: [ring of kFastSlots rows][barriers][fields, log_g, H, spins, active]
-    const size_t row_stride = round16(static_cast<size_t>(v.ld) * sizeof(JT));
-    const size_t bars_at = kFastSlots * row_stride;
-    const size_t base_at = bars_at + round16(kFastSlots * 8);
-    const SmemLayout L = smem_layout(v.ld, v.max_window_bins, true, false);
-    unsigned char* base = smem + base_at;
-    const JT* ring_rows = reinterpret_cast<const JT*>(smem);
-    double* f = reinterpret_cast<double*>(base + L.fields);
+    // carve-up: [kQueue + 1 row slots][draw queue][fields, log_g, H, spins, active]
+    const int ld = v.ld;
+    const size_t row_stride = static_cast<size_t>(ld) * 8;
+    double* ring = reinterpret_cast<double*>(smem);
+    uint64_t* dq = reinterpret_cast<uint64_t*>(smem + (kQueue + 1) * row_stride);
+    unsigned char* base = smem + (kQueue + 1) * row_stride + (kQueueMask + 1) * 8;
+    const SmemLayout L = smem_layout(ld, v.max_window_bins, true, false);
+    double* f_s = reinterpret_cast<double*>(base + L.fields);
     double* lg_s = reinterpret_cast<double*>(base + L.log_g);
     uint64_t* h_s = reinterpret_cast<uint64_t*>(base + L.hist);
     int8_t* sp_s = reinterpret_cast<int8_t*>(base + L.spins);
@@ -507,8 +506,8 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, W
     WalkerState st = v.ws[w];
     const int wb = v.win_begin[st.window], we = v.win_end[st.window], nbins = we - wb;
     const size_t boff = static_cast<size_t>(w) * static_cast<size_t>(v.grid.count) + static_cast<size_t>(wb);
-    double* fg = v.fields + static_cast<size_t>(st.slot) * v.ld;
-    int8_t* sg = v.spins + static_cast<size_t>(st.slot) * v.ld;
+    double2* fg2 = reinterpret_cast<double2*>(v.fields + static_cast<size_t>(st.slot) * ld);
+    int8_t* sg = v.spins + static_cast<size_t>(st.slot) * ld;
     const DeviceParams& P = v.p;
     if (st.cur_bin < wb || st.cur_bin >= we) {  // "Walker escaped its energy window"
         if (lane == 0) record_error(ctl, WLG_ERR_ESCAPED, w);
@@ -524,49 +523,46 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, W
         batch = static_cast<uint32_t>(b < 0xffffffffULL ? b : 0xffffffffULL);
     }
 
-    const JT* J = kPrec == WLG_PRECISION_FP64   ? reinterpret_cast<const JT*>(v.J64)
-                  : kPrec == WLG_PRECISION_FP32 ? reinterpret_cast<const JT*>(v.J32)
-                                                : reinterpret_cast<const JT*>(v.J16);
-    const uint32_t row_bytes = static_cast<uint32_t>(v.ld * sizeof(JT));
-    const uint32_t rs = static_cast<uint32_t>(row_stride);
-    const uint32_t ring_addr = smem_addr(smem);
-    const uint32_t bar_addr = smem_addr(smem + bars_at);
-    if (lane == 0) {
-        for (int s = 0; s < kFastSlots; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_addr + 8 * s) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncwarp();
     const FastMod fm = v.site_mod;
-    Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};
-    uint64_t q0 = rng.next(), q1 = rng.next(), q2 = rng.next(), q3 = rng.next();
-    uint64_t q4 = rng.next(), q5 = rng.next(), q6 = rng.next(), q7 = rng.next();
-    {
-        const uint64_t qs[kFastSlots] = {q0, q1, q2, q3, q4, q5, q6, q7};
+    const double2* J2 = reinterpret_cast<const double2*>(v.J64);
+    const int ld2 = ld >> 1;  // 16-byte chunks per row
+    const uint32_t ring_addr = smem_addr(smem);
+    const uint32_t rs = static_cast<uint32_t>(row_stride);
+    // lane's chunks of a row: c = lane + 32k for k < kChunks, present when c < ld2
+    auto copy_row = [&](uint32_t slot_addr, int site, uint32_t bytes) {
+        const double2* src = J2 + static_cast<size_t>(site) * ld2;
 #pragma unroll
-        for (int s = 0; s < kFastSlots; ++s)
-            issue_row(ring_addr + s * rs, J + fast_mod(fm, qs[s]) * v.ld, row_bytes, bar_addr + 8 * s, false);
-    }
-    uint32_t parity = 0;  // bit s: the phase parity the next wait on slot s expects
-    uint32_t head = 0;    // slot of q0
-    bool failed = false;
-    // Every slot has exactly one copy in flight except between its wait and its refill.
-    auto wait_slot = [&](uint32_t s) -> bool {
-        const uint32_t bar = bar_addr + 8 * s, par = (parity >> s) & 1u;
-        if (!__all_sync(kFull, mbar_try(bar, par)))
-            if (!mbar_wait(bar, par)) return false;
-        parity ^= 1u << s;
-        return true;
+        for (int k = 0; k < kChunks; ++k) {
+            const int c = lane + 32 * k;
+            if (c < ld2) cp_async16(slot_addr + 16u * c, src + c, bytes);
+        }
     };
+    Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};
+    if (lane == 0)
+        for (int k = 0; k < kQueue; ++k) dq[k] = 0;
+    uint64_t first[kQueue];
+#pragma unroll
+    for (int k = 0; k < kQueue; ++k) {
+        first[k] = rng.next();
+        copy_row(ring_addr + k * rs, static_cast<int>(fast_mod(fm, first[k])), 16);
+        cp_async_commit();
+    }
+    if (lane == 0)
+        for (int k = 0; k < kQueue; ++k) dq[k] = first[k];
 
-    // stage the walker (overlaps the first copies)
+    // stage the walker: fields in registers (lane's chunks) and written through to smem
+    double2 fr[kChunks];
+    double2* f2s = reinterpret_cast<double2*>(f_s);
+#pragma unroll
+    for (int k = 0; k < kChunks; ++k) {
+        const int c = lane + 32 * k;
+        fr[k] = c < ld2 ? fg2[c] : make_double2(0.0, 0.0);
+        if (c < ld2) f2s[c] = fr[k];
+    }
     {
-        const double2* src = reinterpret_cast<const double2*>(fg);
-        double2* dst = reinterpret_cast<double2*>(f);
-        for (int k = lane; k < (v.ld >> 1); k += 32) dst[k] = src[k];
         const int4* ssrc = reinterpret_cast<const int4*>(sg);
         int4* sdst = reinterpret_cast<int4*>(sp_s);
-        for (int k = lane; k < (v.ld >> 4); k += 32) sdst[k] = ssrc[k];
+        for (int k = lane; k < (ld >> 4); k += 32) sdst[k] = ssrc[k];
     }
     for (int b = lane; b < nbins; b += 32) {
         lg_s[b] = v.log_g[boff + b];
@@ -590,34 +586,43 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, W
     double factor_next = factor;
     if (stage == kInverseTime && active_count != 0)
         factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + 1);
+    const uint32_t spare_addr = ring_addr + kQueue * rs;
 
-    int i = static_cast<int>(fast_mod(fm, q0));
+    uint32_t hq = 0;  // absolute queue index of the current site draw; its row is in slot hq % kQueue
+    int i = static_cast<int>(fast_mod(fm, dq[0]));
     int si = sp_s[i];
-    double h = f[i];
+    double h = f_s[i];
+    uint64_t q0 = dq[0];
 
     for (uint32_t t = 0; t < batch;) {
-        if (q0 < threshold) {  // rare: bounded() rejects this draw, the next one is the site
-            if (!wait_slot(head)) { failed = true; break; }
-            q0 = q1; q1 = q2; q2 = q3; q3 = q4; q4 = q5; q5 = q6; q6 = q7; q7 = rng.next();
-            issue_row(ring_addr + head * rs, J + fast_mod(fm, q7) * v.ld, row_bytes, bar_addr + 8 * head, false);
-            head = (head + 1) & (kFastSlots - 1);
+        if (q0 < threshold) {  // rare: bounded() rejects this draw; the next one is the site
+            cp_async_wait<0>();
             __syncwarp();
+            const uint64_t d = rng.next();
+            if (lane == 0) dq[(hq + kQueue) & kQueueMask] = d;
+            copy_row(ring_addr + (hq & (kQueue - 1)) * rs, static_cast<int>(fast_mod(fm, d)), 16);
+            cp_async_commit();
+            ++hq;
+            __syncwarp();
+            q0 = dq[hq & kQueueMask];
             i = static_cast<int>(fast_mod(fm, q0));
             si = sp_s[i];
-            h = f[i];
+            h = f_s[i];
             continue;
         }
-        if (!wait_slot(head)) { failed = true; break; }  // the current site's row is resident
-        const JT* row = ring_rows + static_cast<size_t>(head) * (row_stride / sizeof(JT));
+        const uint32_t slot = hq & (kQueue - 1);
+        const double* row = ring + static_cast<size_t>(slot) * ld;
+        const uint64_t q1 = dq[(hq + 1) & kQueueMask];
+        const uint64_t q2 = dq[(hq + 2) & kQueueMask];
+        cp_async_wait<3>();  // the site's row (and the previous attempt's field writes) are in
+        __syncwarp();
         // lookahead: the two candidates for the next site
         const int c1 = static_cast<int>(fast_mod(fm, q1)), c2 = static_cast<int>(fast_mod(fm, q2));
-        const double f1 = f[c1], f2 = f[c2];
+        const double f1 = f_s[c1], f2 = f_s[c2];
         const int s1 = sp_s[c1], s2 = sp_s[c2];
-        const double r1 = jval(row[c1]), r2 = jval(row[c2]);
+        const double r1 = row[c1], r2 = row[c2];
         const double up = fmax(to_uniform(q1), 0x1.0p-53);
         const double est = static_cast<double>(__log2f(static_cast<float>(up))) * 0.6931471805599453;
-        double scale = 1.0;
-        if constexpr (kPrec == WLG_PRECISION_BF16) scale = static_cast<double>(__ldg(v.Jscale + i));
 
         // the decision (attempt_flip, src/wang_landau.cpp:244-262)
         const double m = si > 0 ? -2.0 : 2.0;  // -2 * spin
@@ -640,12 +645,22 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, W
 
         // the next attempt's site, field and spin
         const int c = need_u ? c2 : c1;
-        const double m_eff = (accepted ? m : 0.0) * scale;
+        const double m_eff = accepted ? m : 0.0;
         const double h_next = fma(m_eff, need_u ? r2 : r1, need_u ? f2 : f1);
         const int s_next = (accepted && c == i) ? -si : (need_u ? s2 : s1);
 
-        // add_flip_delta, off the chain (m_eff = 0 leaves every field unchanged)
-        row_update<kPrec>(row, v.ld, m_eff, f, lane);
+        // add_flip_delta off the chain (m_eff = 0 leaves every field unchanged)
+        const double2* row2 = reinterpret_cast<const double2*>(row);
+#pragma unroll
+        for (int k = 0; k < kChunks; ++k) {
+            const int cc = lane + 32 * k;
+            if (cc < ld2) {
+                const double2 r = row2[cc];
+                fr[k].x = fma(m_eff, r.x, fr[k].x);
+                fr[k].y = fma(m_eff, r.y, fr[k].y);
+                f2s[cc] = fr[k];
+            }
+        }
         if (lane == 0 && accepted) sp_s[i] = static_cast<int8_t>(-si);
         E = accepted ? Ep : E;
         since = accepted ? 0 : since + 1;
@@ -674,42 +689,34 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, W
         if (stage == kInverseTime && active_count != 0)
             factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + t + 1);
 
-        // ring: the site draw (and the uniform, when used) leave; their slots get new draws
-        const uint32_t sA = head, sB = (head + 1) & (kFastSlots - 1);
-        if (need_u) {
-            if (!wait_slot(sB)) { failed = true; break; }
-        }
+        // the consumed draws leave the queue; their slots get the draws kQueue ahead
         const uint64_t d1 = rng.next();
         Rng r2n = rng;
         const uint64_t d2 = r2n.next();
-        if (need_u) rng = r2n;
-        __syncwarp();  // all lanes' reads of the site's row precede its refill
-        // d1 lands in the site's slot; d2 (only when the uniform was used) in the uniform's
-        issue_rows(ring_addr + sA * rs, J + fast_mod(fm, d1) * v.ld, bar_addr + 8 * sA, ring_addr + sB * rs,
-                   J + fast_mod(fm, d2) * v.ld, bar_addr + 8 * sB, row_bytes, need_u);
+        rng.s0 = need_u ? r2n.s0 : rng.s0;
+        rng.s1 = need_u ? r2n.s1 : rng.s1;
+        rng.s2 = need_u ? r2n.s2 : rng.s2;
+        rng.s3 = need_u ? r2n.s3 : rng.s3;
+        if (lane == 0) {
+            dq[(hq + kQueue) & kQueueMask] = d1;
+            dq[(hq + kQueue + 1) & kQueueMask] = d2;
+        }
+        cp_async_wait<2>();  // the next draw's slot is free to reuse when the uniform was consumed
+        __syncwarp();        // every lane has read the site's row and written its fields
+        copy_row(ring_addr + slot * rs, static_cast<int>(fast_mod(fm, d1)), 16);
+        copy_row(need_u ? ring_addr + ((hq + 1) & (kQueue - 1)) * rs : spare_addr, static_cast<int>(fast_mod(fm, d2)),
+                 need_u ? 16u : 0u);
+        cp_async_commit();
+        hq += need_u ? 2u : 1u;
         q0 = need_u ? q2 : q1;
-        q1 = need_u ? q3 : q2;
-        q2 = need_u ? q4 : q3;
-        q3 = need_u ? q5 : q4;
-        q4 = need_u ? q6 : q5;
-        q5 = need_u ? q7 : q6;
-        q6 = need_u ? d1 : q7;
-        q7 = need_u ? d2 : d1;
-        head = (head + (need_u ? 2u : 1u)) & (kFastSlots - 1);
         i = c;
         si = s_next;
         h = h_next;
-        __syncwarp();
     }
-    for (uint32_t s = 0; s < kFastSlots; ++s)  // drain: no copy may land after the CTA exits
-        if (!wait_slot(s)) failed = true;
-    if (failed) {
-        if (lane == 0) record_error(ctl, WLG_ERR_TIMEOUT, w);
-        return;
-    }
+    cp_async_wait<0>();  // no copy may land after the CTA exits
     if (lane == 0) lg_s[cur - wb] = lg_cur;
     __syncwarp();
-    for (int k = 0; k < kFastSlots; ++k) rng_step_back(rng);  // back over the queued draws
+    for (int k = 0; k < kQueue; ++k) rng_step_back(rng);  // back over the queued draws
 
     st.rng[0] = rng.s0;
     st.rng[1] = rng.s1;
@@ -734,13 +741,15 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, W
             if (stats_ready(hs, st.stage, P)) warp_begin_next_iteration(st, h_s, nullptr, nbins, P, lane);
         }
     }
+#pragma unroll
+    for (int k = 0; k < kChunks; ++k) {
+        const int c = lane + 32 * k;
+        if (c < ld2) fg2[c] = fr[k];
+    }
     {
-        const double2* src = reinterpret_cast<const double2*>(f);
-        double2* dst = reinterpret_cast<double2*>(fg);
-        for (int k = lane; k < (v.ld >> 1); k += 32) dst[k] = src[k];
         const int4* ssrc = reinterpret_cast<const int4*>(sp_s);
         int4* sdst = reinterpret_cast<int4*>(sg);
-        for (int k = lane; k < (v.ld >> 4); k += 32) sdst[k] = ssrc[k];
+        for (int k = lane; k < (ld >> 4); k += 32) sdst[k] = ssrc[k];
     }
     for (int b = lane; b < nbins; b += 32) {
         v.log_g[boff + b] = lg_s[b];
@@ -756,8 +765,8 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, W
     }
 }
 
-size_t fast_smem_bytes(const EngineView& v, size_t jbytes) {
-    return kFastSlots * round16(static_cast<size_t>(v.ld) * jbytes) + round16(kFastSlots * 8) +
+size_t fast_smem_bytes(const EngineView& v) {
+    return (kQueue + 1) * static_cast<size_t>(v.ld) * 8 + (kQueueMask + 1) * 8 +
            smem_layout(v.ld, v.max_window_bins, true, false).total;
 }
 
@@ -777,27 +786,48 @@ SweepFn sweep_fn() {
 
 }  // namespace
 
-template <int P>
+template <int K>
 SweepFn fast_fn() {
     static bool configured = false;
     if (!configured) {
-        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_dense_fast_kernel<P>),
+        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_dense_fast_kernel<K>),
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
                    "cudaFuncSetAttribute");
         configured = true;
     }
-    return &sweep_dense_fast_kernel<P>;
+    return &sweep_dense_fast_kernel<K>;
+}
+
+// The lookahead sweep for FP64 couplings with ld <= 1024 (chunks of 64 doubles per lane pass).
+SweepFn pick_fast(int ld) {
+    switch ((ld + 63) / 64) {
+        case 1: return fast_fn<1>();
+        case 2: return fast_fn<2>();
+        case 3: return fast_fn<3>();
+        case 4: return fast_fn<4>();
+        case 5: return fast_fn<5>();
+        case 6: return fast_fn<6>();
+        case 7: return fast_fn<7>();
+        case 8: return fast_fn<8>();
+        case 9: return fast_fn<9>();
+        case 10: return fast_fn<10>();
+        case 11: return fast_fn<11>();
+        case 12: return fast_fn<12>();
+        case 13: return fast_fn<13>();
+        case 14: return fast_fn<14>();
+        case 15: return fast_fn<15>();
+        case 16: return fast_fn<16>();
+        default: return nullptr;
+    }
 }
 
 bool launch_sweep_dense(const EngineView& v, const WalkArgs& a, cudaStream_t stream) {
     const bool features = v.p.collect || v.p.nalivaiko;
     const size_t jbytes = v.precision == WLG_PRECISION_FP64 ? 8 : v.precision == WLG_PRECISION_FP32 ? 4 : 2;
-    if (!features) {  // the lookahead sweep
-        const size_t fast_bytes = fast_smem_bytes(v, jbytes);
-        if (fast_bytes <= 227 * 1024) {
-            SweepFn fn = v.precision == WLG_PRECISION_FP32   ? fast_fn<WLG_PRECISION_FP32>()
-                         : v.precision == WLG_PRECISION_BF16 ? fast_fn<WLG_PRECISION_BF16>()
-                                                             : fast_fn<WLG_PRECISION_FP64>();
+    if (!features && v.precision == WLG_PRECISION_FP64 && v.ld <= 1024) {  // the lookahead sweep
+        const size_t fast_bytes = fast_smem_bytes(v);
+        SweepFn fn = pick_fast(v.ld);
+        if (fn && fast_bytes <= 227 * 1024) {
             fn<<<static_cast<unsigned>(a.count), 32, fast_bytes, stream>>>(v, a);
             check_cuda(cudaGetLastError(), "sweep_dense_fast_kernel");
             return true;
