@@ -22,6 +22,8 @@
 //
 // The arithmetic is the reference's, operation for operation (see walker.cu for the shared
 // argument about fma(m, J, h) with m = +-2 and the power-of-two bin width).
+#include <type_traits>
+
 #include "engine.hpp"
 #include "walker_dev.cuh"
 
@@ -443,76 +445,128 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_kernel(EngineView v, WalkAr
     }
 }
 
-// ---- the lookahead sweep (FP64 couplings, no pilot statistics, no Nalivaiko mask) --------
+// ---- the split sweep (FP64 couplings, no pilot statistics, no Nalivaiko mask) ------------
 //
-// The same attempt as above, reorganised so that the N-element field update is not on the
-// path from one attempt to the next, and so that the loop body is one branch-free block the
-// compiler can schedule freely:
+// The same attempts as sweep_dense_kernel, with the work that does not depend on the walk
+// moved to a second warp of the CTA, which the SM runs on another scheduler:
 //
-// * The next attempt's site is the draw after the site draw (q1) or, when this attempt
-//   consumes the acceptance uniform, the one after that (q2).  Before deciding, the warp
-//   loads for both candidates their field, spin and the J entry of the current site's row;
-//   after deciding it forms the next attempt's field with one fma.
-// * The update of all N fields then runs off the chain with m_eff = accepted ? m : 0: adding
-//   m*0 changes no field, because a field is never -0.0 (sums start at +0.0 and a sum that
-//   reaches zero is +0.0), so the fields stay bit-identical to the reference's.  Each lane
-//   keeps its share of the fields in registers and writes them through to shared memory,
-//   where the random single-field reads find them.
-// * Rows arrive by per-lane cp.async copies, one commit group per attempt: each lane copies
-//   exactly the 16-byte chunks of the row it will update.  A draw appended to the queue
-//   reaches its head no earlier than four attempts later (it enters at position >= 6 and
-//   moves by at most 2 per attempt), so "all but the 3 newest groups complete" covers the
-//   site's row and "all but the 2 newest" the next draw's slot before it is reused; both
-//   waits are single instructions.  When the uniform is not consumed, the second copy of the
-//   attempt is a zero-size copy into a spare slot, so every attempt commits exactly one group.
-// * The draws live in a small shared-memory queue; the generator runs kQueue draws ahead and
-//   is stepped back over them at the end of the batch.
-// Rare events (a rejected bounded() draw, an acceptance test inside the log margin, a first
-// visit of a bin) take branches.
+// * Warp 1 (the producer) generates the walker's draws in batches of kDrawBatch.  Every lane
+//   steps the generator through the batch and lane j keeps draw j; for it, lane j stores in
+//   ring entry k % Q the site the draw would select (-1 when bounded() rejects it) and
+//   log(max(u, 2^-53)) of the uniform it would give (src/wang_landau.cpp:261), and starts
+//   the bulk copy of that site's J row into the entry's row slot.  The batch's copies
+//   complete one mbarrier.  The producer stays at most Q draws ahead of the walker, which
+//   publishes with a release store, after every attempt, the draws it no longer needs.
+// * Warp 0 (the walker) runs the decision chain and the bookkeeping.  It waits on a batch's
+//   barrier only when its lookahead (up to draw hq+4, hq being the current site's draw)
+//   enters that batch.
+// * The next attempt's site is q1 = draw hq+1 or, when this attempt consumes the acceptance
+//   uniform, q2 = draw hq+2.  The walker loads for both candidates their field, spin and the
+//   J entries it needs before deciding, and after deciding forms the next attempt's field
+//   with one fma.  The update of all N fields (add_flip_delta) is applied one attempt late,
+//   off the chain: during attempt t the lanes add m_{t-1} * row_{t-1} to the fields they keep
+//   in registers and write them through to shared memory at the end of the attempt, so
+//   shared memory holds the fields up to attempt t-2 while t runs; a candidate's field is
+//   then fma(m_t, J_t, fma(m_{t-1}, J_{t-1}, f)), the reference's two updates in order.  An
+//   update with m_eff = 0 (rejected flip) changes no field, because a field is never -0.0
+//   (sums start at +0.0 and a sum that reaches zero is +0.0), so the fields stay
+//   bit-identical to the reference's.
+// * Within an attempt every shared-memory load is issued before every store: a load issued
+//   behind pending stores of the same warp waits for them, which serialised the chain.
+// * Histogram increments go to a 32-bit shared-memory delta per bin (a reduction without
+//   return) that is folded into H at the end of the batch.  In the Wang-Landau stage the
+//   count of active bins is not read during the batch, so it is updated once, from the active
+//   mask, at the end; in the 1/t stage it is maintained per attempt.
+// * At the end of the batch the walker publishes a stop flag; the producer waits for every
+//   copy it started, and the generator is stepped back over the draws the walker did not
+//   consume, so the stored RNG state is the reference's.  All waits are bounded: on timeout
+//   the walker records WLG_ERR_TIMEOUT, the copies are drained (bounded again) and the
+//   walker's state is not written back.
+// Bit-exactness of the rearranged arithmetic: E + (-2s)h is evaluated as fma(m, h, E), equal
+// because m*h (m = +-2) is exact; with a power-of-two bin width, (E' - min) / width is
+// evaluated as fma(E', 1/width, -min/width), equal because scaling by a power of two is exact
+// and commutes with rounding; log(max(u, 2^-53)) < log_ratio is evaluated with the CUDA log,
+// whose result can differ from the C library's only in the last bit.
 
-constexpr int kQueue = 8;       // draws generated ahead; row slots in the ring
-constexpr int kQueueMask = 15;  // shared-memory draw queue of 16 entries
+constexpr uint32_t kProducerPolls = 1u << 24;
+constexpr int kDrawBatch = 4;  // draws per producer batch (one barrier per batch)
+// Ring of 16 draws: the walker reads up to draw hq+4 while it still holds the row of draw
+// hq-1 or hq-2, and the producer must be able to complete the batch holding draw hq+4.
+constexpr int kRingLog = 4;
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+struct SplitLayout {
+    size_t ring, bars, lnu, site, hd, ctl, base, total;
+};
+__host__ __device__ inline SplitLayout split_layout(int ld, int mwb) {
+    constexpr size_t q = size_t{1} << kRingLog;
+    SplitLayout L;
+    size_t at = 0;
+    L.ring = at; at += q * static_cast<size_t>(ld) * 8;
+    L.bars = at; at += round16((q / kDrawBatch) * 8);
+    L.lnu = at; at += round16(q * 8);
+    L.site = at; at += round16(q * 4);
+    L.hd = at; at += round16(static_cast<size_t>(mwb) * 4);
+    L.ctl = at; at += 64;  // consumed, stop, producer status, produced, rng[4]
+    L.base = at; at += smem_layout(ld, mwb, true, false).total;
+    L.total = at;
+    return L;
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int kPending> __device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(kPending) : "memory");
+
+__device__ __forceinline__ void st_release_shared(uint32_t addr, uint32_t value) {
+    asm volatile("st.release.cta.shared::cta.u32 [%0], %1;" ::"r"(addr), "r"(value) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_acquire_shared(uint32_t addr) {
+    uint32_t value;
+    asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(value) : "r"(addr) : "memory");
+    return value;
+}
+// Bounded wait of one thread for the completion of phase `parity` of one barrier.
+__device__ __forceinline__ bool mbar_wait_thread(uint32_t bar, uint32_t parity) {
+    for (uint32_t k = 0; k < kWaitPolls; ++k)
+        if (mbar_try(bar, parity)) return true;
+    return false;
 }
 
-template <int kChunks>
-__global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, WalkArgs a) {
+template <int kChunks, bool kPow2>
+__global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, WalkArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
-    const int lane = threadIdx.x & 31;
+    constexpr int qlog = kRingLog;
+    constexpr uint32_t qm = (1u << qlog) - 1u;
+    constexpr int blog = qlog - 2;  // log2 of the number of batch barriers (kDrawBatch == 4)
+    constexpr uint32_t bm = (1u << blog) - 1u;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (static_cast<int>(blockIdx.x) >= a.count) return;
     const int w = a.first + static_cast<int>(blockIdx.x);
     Control* ctl = v.ctl;
     if (a.epoch_mode && *reinterpret_cast<volatile int32_t*>(&ctl->done)) return;
 
-    // carve-up: [kQueue + 1 row slots][draw queue][fields, log_g, H, spins, active]
     const int ld = v.ld;
-    const size_t row_stride = static_cast<size_t>(ld) * 8;
-    double* ring = reinterpret_cast<double*>(smem);
-    uint64_t* dq = reinterpret_cast<uint64_t*>(smem + (kQueue + 1) * row_stride);
-    unsigned char* base = smem + (kQueue + 1) * row_stride + (kQueueMask + 1) * 8;
+    const SplitLayout SL = split_layout(ld, v.max_window_bins);
     const SmemLayout L = smem_layout(ld, v.max_window_bins, true, false);
+    const double* ring = reinterpret_cast<const double*>(smem + SL.ring);
+    double* rec_lnu = reinterpret_cast<double*>(smem + SL.lnu);
+    int32_t* rec_site = reinterpret_cast<int32_t*>(smem + SL.site);
+    uint32_t* hd = reinterpret_cast<uint32_t*>(smem + SL.hd);
+    uint32_t* sctl = reinterpret_cast<uint32_t*>(smem + SL.ctl);  // [0] consumed [1] stop [2] status [3] produced
+    uint64_t* srng = reinterpret_cast<uint64_t*>(smem + SL.ctl + 32);
+    unsigned char* base = smem + SL.base;
     double* f_s = reinterpret_cast<double*>(base + L.fields);
     double* lg_s = reinterpret_cast<double*>(base + L.log_g);
     uint64_t* h_s = reinterpret_cast<uint64_t*>(base + L.hist);
     int8_t* sp_s = reinterpret_cast<int8_t*>(base + L.spins);
     uint8_t* act_s = base + L.active;
+    const uint32_t ring_addr = smem_addr(smem + SL.ring);
+    const uint32_t bar_addr = smem_addr(smem + SL.bars);
+    const uint32_t consumed_addr = smem_addr(sctl), stop_addr = consumed_addr + 4;
+    const uint32_t row_bytes = static_cast<uint32_t>(ld) * 8u;
 
     WalkerState st = v.ws[w];
     const int wb = v.win_begin[st.window], we = v.win_end[st.window], nbins = we - wb;
-    const size_t boff = static_cast<size_t>(w) * static_cast<size_t>(v.grid.count) + static_cast<size_t>(wb);
-    double2* fg2 = reinterpret_cast<double2*>(v.fields + static_cast<size_t>(st.slot) * ld);
-    int8_t* sg = v.spins + static_cast<size_t>(st.slot) * ld;
-    const DeviceParams& P = v.p;
     if (st.cur_bin < wb || st.cur_bin >= we) {  // "Walker escaped its energy window"
-        if (lane == 0) record_error(ctl, WLG_ERR_ESCAPED, w);
+        if (threadIdx.x == 0) record_error(ctl, WLG_ERR_ESCAPED, w);
         return;
     }
+    const DeviceParams& P = v.p;
     uint32_t batch;
     {
         uint64_t b = a.fixed_batch ? a.fixed_batch : P.exchange_interval;
@@ -522,201 +576,332 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, W
         }
         batch = static_cast<uint32_t>(b < 0xffffffffULL ? b : 0xffffffffULL);
     }
+    const size_t boff = static_cast<size_t>(w) * static_cast<size_t>(v.grid.count) + static_cast<size_t>(wb);
+    double2* fg2 = reinterpret_cast<double2*>(v.fields + static_cast<size_t>(st.slot) * ld);
+    int8_t* sg = v.spins + static_cast<size_t>(st.slot) * ld;
+    const int ld2 = ld >> 1;
+    double2 fr[kChunks];
+    double2* f2s = reinterpret_cast<double2*>(f_s);
 
-    const FastMod fm = v.site_mod;
-    const double2* J2 = reinterpret_cast<const double2*>(v.J64);
-    const int ld2 = ld >> 1;  // 16-byte chunks per row
-    const uint32_t ring_addr = smem_addr(smem);
-    const uint32_t rs = static_cast<uint32_t>(row_stride);
-    // lane's chunks of a row: c = lane + 32k for k < kChunks, present when c < ld2
-    auto copy_row = [&](uint32_t slot_addr, int site, uint32_t bytes) {
-        const double2* src = J2 + static_cast<size_t>(site) * ld2;
+    if (warp == 1) {
+        if (lane == 0) {
+            for (uint32_t s = 0; s <= bm; ++s)
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_addr + 8 * s) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            sctl[0] = 0;
+            sctl[1] = 0;
+            sctl[2] = 0;
+        }
+        for (int b = lane; b < nbins; b += 32) hd[b] = 0;
+    } else {
+        // stage the walker: fields in registers (lane's chunks) and written through to smem
 #pragma unroll
         for (int k = 0; k < kChunks; ++k) {
             const int c = lane + 32 * k;
-            if (c < ld2) cp_async16(slot_addr + 16u * c, src + c, bytes);
+            fr[k] = c < ld2 ? fg2[c] : make_double2(0.0, 0.0);
+            if (c < ld2) f2s[c] = fr[k];
         }
-    };
-    Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};
-    if (lane == 0)
-        for (int k = 0; k < kQueue; ++k) dq[k] = 0;
-    uint64_t first[kQueue];
-#pragma unroll
-    for (int k = 0; k < kQueue; ++k) {
-        first[k] = rng.next();
-        copy_row(ring_addr + k * rs, static_cast<int>(fast_mod(fm, first[k])), 16);
-        cp_async_commit();
-    }
-    if (lane == 0)
-        for (int k = 0; k < kQueue; ++k) dq[k] = first[k];
-
-    // stage the walker: fields in registers (lane's chunks) and written through to smem
-    double2 fr[kChunks];
-    double2* f2s = reinterpret_cast<double2*>(f_s);
-#pragma unroll
-    for (int k = 0; k < kChunks; ++k) {
-        const int c = lane + 32 * k;
-        fr[k] = c < ld2 ? fg2[c] : make_double2(0.0, 0.0);
-        if (c < ld2) f2s[c] = fr[k];
-    }
-    {
         const int4* ssrc = reinterpret_cast<const int4*>(sg);
         int4* sdst = reinterpret_cast<int4*>(sp_s);
         for (int k = lane; k < (ld >> 4); k += 32) sdst[k] = ssrc[k];
+        for (int b = lane; b < nbins; b += 32) {
+            lg_s[b] = v.log_g[boff + b];
+            h_s[b] = v.hist[boff + b];
+            act_s[b] = v.active[boff + b];
+        }
     }
-    for (int b = lane; b < nbins; b += 32) {
-        lg_s[b] = v.log_g[boff + b];
-        h_s[b] = v.hist[boff + b];
-        act_s[b] = v.active[boff + b];
-    }
-    __syncwarp();
+    __syncthreads();
 
+    if (warp == 1) {
+        // ---- producer: batches of kDrawBatch draws, lane j < kDrawBatch handles draw j ----
+        const FastMod fm = v.site_mod;
+        const double* J = v.J64;
+        Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};
+        uint32_t produced = 0, status = 0;
+        for (;;) {
+            uint32_t consumed = __shfl_sync(kFull, lane == 0 ? ld_acquire_shared(consumed_addr) : 0u, 0);
+            if (produced + kDrawBatch - consumed > qm + 1) {  // no room for a batch yet
+                uint32_t go = 0;
+                if (lane == 0) {
+                    for (uint32_t polls = 0; polls < kProducerPolls; ++polls) {
+                        if (ld_acquire_shared(stop_addr)) break;
+                        consumed = ld_acquire_shared(consumed_addr);
+                        if (produced + kDrawBatch - consumed <= qm + 1) {
+                            go = 1;
+                            break;
+                        }
+                    }
+                    if (!go && !ld_acquire_shared(stop_addr)) status = WLG_ERR_TIMEOUT;
+                }
+                if (!__shfl_sync(kFull, go, 0)) break;
+            }
+            __syncwarp();  // lane 0's acquire orders the walker's reads before this batch's writes
+            uint64_t mine = 0;
+#pragma unroll
+            for (int j = 0; j < kDrawBatch; ++j) {
+                const uint64_t d = rng.next();
+                mine = lane == j ? d : mine;
+            }
+            const uint32_t k = produced + static_cast<uint32_t>(lane);
+            const uint32_t e = k & qm;
+            int site = 0;
+            if (lane < kDrawBatch) {
+                site = mine < fm.threshold ? -1 : static_cast<int>(fast_mod(fm, mine));
+                rec_lnu[e] = log(fmax(to_uniform(mine), 0x1.0p-53));
+                rec_site[e] = site;
+            }
+            const uint32_t n = produced >> 2;  // batch index
+            const uint32_t bar = bar_addr + 8 * (n & bm);
+            __syncwarp();  // the batch's records are written before its barrier is armed
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                             "r"(row_bytes * kDrawBatch)
+                             : "memory");
+            __syncwarp();
+            if (lane < kDrawBatch) {
+                const double* src = J + static_cast<size_t>(site < 0 ? 0 : site) * ld;
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        ring_addr + e * row_bytes),
+                    "l"(src), "r"(row_bytes), "r"(bar)
+                    : "memory");
+            }
+            produced += kDrawBatch;
+        }
+        // every copy started must land before the block exits: the latest batch of each
+        // barrier is the only one whose copies can still be in flight
+        if (lane == 0) {
+            const uint32_t batches = produced >> 2;
+            const uint32_t first = batches > bm ? batches - bm - 1 : 0;
+            for (uint32_t n = first; n != batches; ++n)
+                if (!mbar_wait_thread(bar_addr + 8 * (n & bm), (n >> blog) & 1u)) status = WLG_ERR_TIMEOUT;
+            sctl[2] = status;
+            sctl[3] = produced;
+            srng[0] = rng.s0;
+            srng[1] = rng.s1;
+            srng[2] = rng.s2;
+            srng[3] = rng.s3;
+        }
+        __syncthreads();
+        return;
+    }
+
+    // ---- walker ----
     double E = st.energy;
     double factor = st.factor;
     int32_t stage = st.stage;
     const uint64_t att0 = st.attempted;
     uint64_t since = st.attempted - st.last_accepted;
+    const uint64_t force_limit = P.force_after != 0 ? P.force_after : ~0ULL;
     uint32_t n_acc = 0, n_forced = 0;
     uint64_t active_count = st.active_count;
     const Grid g = v.grid;
     const int gcount = static_cast<int>(g.count);
+    const double neg_min_scaled = -g.minimum * g.inv_width;
     int cur = st.cur_bin;
     double lg_cur = lg_s[cur - wb];
-    const uint64_t threshold = fm.threshold;
-    double factor_next = factor;
-    if (stage == kInverseTime && active_count != 0)
-        factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + 1);
-    const uint32_t spare_addr = ring_addr + kQueue * rs;
+    bool failed = false;
 
-    uint32_t hq = 0;  // absolute queue index of the current site draw; its row is in slot hq % kQueue
-    int i = static_cast<int>(fast_mod(fm, dq[0]));
-    int si = sp_s[i];
-    double h = f_s[i];
-    uint64_t q0 = dq[0];
-
-    for (uint32_t t = 0; t < batch;) {
-        if (q0 < threshold) {  // rare: bounded() rejects this draw; the next one is the site
-            cp_async_wait<0>();
-            __syncwarp();
-            const uint64_t d = rng.next();
-            if (lane == 0) dq[(hq + kQueue) & kQueueMask] = d;
-            copy_row(ring_addr + (hq & (kQueue - 1)) * rs, static_cast<int>(fast_mod(fm, d)), 16);
-            cp_async_commit();
-            ++hq;
-            __syncwarp();
-            q0 = dq[hq & kQueueMask];
-            i = static_cast<int>(fast_mod(fm, q0));
+    uint32_t hq = 0;        // draw index of the current site
+    uint32_t ready_to = 0;  // draws [0, ready_to) are known to be in shared memory
+    // make draws [0, need] available (false on timeout)
+    auto ensure = [&](uint32_t need) -> bool {
+        while (static_cast<int32_t>(need - ready_to) >= 0) {
+            const uint32_t n = ready_to >> 2;
+            if (!__all_sync(kFull, mbar_wait_thread(bar_addr + 8 * (n & bm), (n >> blog) & 1u))) return false;
+            ready_to += kDrawBatch;
+        }
+        return true;
+    };
+    if (!ensure(4)) failed = true;
+    int i = -1, si = 0, c1 = -1, c2 = -1;  // current site; candidates for the next one
+    double h = 0.0, lnu = 0.0;             // field of the current site; log uniform of draw hq+1
+    if (!failed) {
+        i = rec_site[0];
+        c1 = rec_site[1];
+        c2 = rec_site[2];
+        lnu = rec_lnu[1];
+        if (i >= 0) {
             si = sp_s[i];
             h = f_s[i];
-            continue;
         }
-        const uint32_t slot = hq & (kQueue - 1);
-        const double* row = ring + static_cast<size_t>(slot) * ld;
-        const uint64_t q1 = dq[(hq + 1) & kQueueMask];
-        const uint64_t q2 = dq[(hq + 2) & kQueueMask];
-        cp_async_wait<3>();  // the site's row (and the previous attempt's field writes) are in
-        __syncwarp();
-        // lookahead: the two candidates for the next site
-        const int c1 = static_cast<int>(fast_mod(fm, q1)), c2 = static_cast<int>(fast_mod(fm, q2));
-        const double f1 = f_s[c1], f2 = f_s[c2];
-        const int s1 = sp_s[c1], s2 = sp_s[c2];
-        const double r1 = row[c1], r2 = row[c2];
-        const double up = fmax(to_uniform(q1), 0x1.0p-53);
-        const double est = static_cast<double>(__log2f(static_cast<float>(up))) * 0.6931471805599453;
+    }
+    // The field update of an attempt is applied during the next one: m_prev and prev_slot
+    // are its factor and row.  Shared memory holds the fields up to the attempt before.
+    double m_prev = 0.0;
+    uint32_t prev_slot = 0;
+    uint64_t active_before = 0;
+    if (stage != kInverseTime) {
+        for (int b = lane; b < nbins; b += 32) active_before += act_s[b] ? 1 : 0;
+        active_before = warp_sum_u64(active_before);
+    }
 
-        // the decision (attempt_flip, src/wang_landau.cpp:244-262)
-        const double m = si > 0 ? -2.0 : 2.0;  // -2 * spin
-        const double delta = m * h;
-        const double Ep = E + delta;
-        const double off = Ep - g.minimum;
-        const double qv = g.pow2_width ? off * g.inv_width : off / g.width;
-        int nb = (Ep >= g.minimum && Ep <= g.maximum) ? __double2int_rd(qv) : -1;
-        nb = (nb == gcount && Ep == g.maximum) ? gcount - 1 : nb;
-        const bool in_window = nb >= wb && nb < we;
-        const double lg_load = lg_s[in_window ? nb - wb : 0];
-        const double lg_new = nb == cur ? lg_cur : lg_load;
-        const double log_ratio = lg_cur - lg_new;
-        const bool det = log_ratio >= 0.0;
-        const bool forced = !det && P.force_after != 0 && since >= P.force_after;
-        const bool need_u = in_window && !det && !forced;
-        bool u_ok = est < log_ratio - 1e-3;
-        if (need_u && !u_ok && !(est > log_ratio + 1e-3)) u_ok = log(up) < log_ratio;  // inside the margin
-        const bool accepted = in_window && (det || forced || u_ok);
+    // The attempts of one batch; kIT selects the 1/t stage (per-attempt factor and active
+    // count) or the Wang-Landau / frozen stages (constant factor).
+    auto run = [&](auto it_tag) {
+        constexpr bool kIT = decltype(it_tag)::value;
+        const bool frozen = stage == kFrozen;
+        double factor_next = factor;
+        if (kIT && active_count != 0) factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + 1);
+        for (uint32_t t = 0; t < batch;) {
+            if (static_cast<int32_t>(hq + 4 - ready_to) >= 0 && !ensure(hq + 4)) {
+                failed = true;
+                break;
+            }
+            const double* prow = ring + static_cast<size_t>(prev_slot) * ld;
+            if (i < 0) {  // rare: bounded() rejects draw hq; the next draw is the candidate site
+                hq += 1;
+                i = c1;
+                if (i >= 0) {
+                    si = sp_s[i];
+                    h = fma(m_prev, prow[i], f_s[i]);
+                }
+                c1 = c2;
+                c2 = rec_site[(hq + 2) & qm];
+                lnu = rec_lnu[(hq + 1) & qm];
+                continue;
+            }
+            const uint32_t slot = hq & qm;
+            const double* row = ring + static_cast<size_t>(slot) * ld;
+            // loads: the next attempt's records, the candidates' fields, spins and couplings,
+            // the previous attempt's row
+            const int r3 = rec_site[(hq + 3) & qm], r4 = rec_site[(hq + 4) & qm];
+            const double l2 = rec_lnu[(hq + 2) & qm], l3 = rec_lnu[(hq + 3) & qm];
+            const int c1l = c1 < 0 ? 0 : c1, c2l = c2 < 0 ? 0 : c2;
+            const double f1 = f_s[c1l], f2 = f_s[c2l];
+            const int s1 = sp_s[c1l], s2 = sp_s[c2l];
+            const double r1 = row[c1l], r2 = row[c2l];
+            const double p1 = prow[c1l], p2 = prow[c2l];
+            const double2* prow2 = reinterpret_cast<const double2*>(prow);
+            double2 rb[kChunks];
+#pragma unroll
+            for (int k = 0; k < kChunks; ++k) {
+                const int cc = lane + 32 * k;
+                rb[k] = cc < ld2 ? prow2[cc] : make_double2(0.0, 0.0);
+            }
+            // the previous attempt's add_flip_delta (m_prev = 0 leaves every field unchanged)
+#pragma unroll
+            for (int k = 0; k < kChunks; ++k) {
+                fr[k].x = fma(m_prev, rb[k].x, fr[k].x);
+                fr[k].y = fma(m_prev, rb[k].y, fr[k].y);
+            }
+            const double fc1 = fma(m_prev, p1, f1), fc2 = fma(m_prev, p2, f2);
 
-        // the next attempt's site, field and spin
-        const int c = need_u ? c2 : c1;
-        const double m_eff = accepted ? m : 0.0;
-        const double h_next = fma(m_eff, need_u ? r2 : r1, need_u ? f2 : f1);
-        const int s_next = (accepted && c == i) ? -si : (need_u ? s2 : s1);
+            // the decision (attempt_flip, src/wang_landau.cpp:244-262)
+            const double m = si > 0 ? -2.0 : 2.0;  // -2 * spin
+            const double Ep = fma(m, h, E);
+            const bool in_range = Ep >= g.minimum && Ep <= g.maximum;
+            const double qv = kPow2 ? fma(Ep, g.inv_width, neg_min_scaled) : (Ep - g.minimum) / g.width;
+            int nb = in_range ? __double2int_rd(qv) : -1;
+            nb = (nb == gcount && Ep == g.maximum) ? gcount - 1 : nb;
+            const bool in_window = nb >= wb && nb < we;
+            const double lg_load = lg_s[in_window ? nb - wb : 0];
+            const double lg_new = nb == cur ? lg_cur : lg_load;
+            const double log_ratio = lg_cur - lg_new;
+            const bool det = log_ratio >= 0.0;
+            const bool forced = !det && since >= force_limit;
+            const bool need_u = in_window && !det && !forced;
+            const bool accepted = in_window && (det || forced || lnu < log_ratio);
 
-        // add_flip_delta off the chain (m_eff = 0 leaves every field unchanged)
-        const double2* row2 = reinterpret_cast<const double2*>(row);
+            // the next attempt's site, field and spin
+            const int c = need_u ? c2 : c1;
+            const double m_eff = accepted ? m : 0.0;
+            const double h_next = fma(m_eff, need_u ? r2 : r1, need_u ? fc2 : fc1);
+            const int s_next = (accepted && c == i) ? -si : (need_u ? s2 : s1);
+            E = accepted ? Ep : E;
+            since = accepted ? 0 : since + 1;
+            n_acc += accepted ? 1u : 0u;
+            n_forced += (accepted && forced) ? 1u : 0u;
+            ++t;
+
+            // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
+            if (kIT && stage == kInverseTime) {
+                factor = factor_next;
+                if (factor <= P.final_factor) stage = kFrozen;
+            }
+            const bool move = accepted && nb != cur;
+            const int ncur = move ? nb : cur;
+            const double lg_base = move ? lg_new : lg_cur;
+            if (kIT) {
+                const bool visited = act_s[ncur - wb] != 0;
+                active_count += visited ? 0 : 1;
+            }
+
+            // stores: the fields up to the previous attempt, the flipped spin, log g of the
+            // bin left behind, the visit
+#pragma unroll
+            for (int k = 0; k < kChunks; ++k) {
+                const int cc = lane + 32 * k;
+                if (cc < ld2) f2s[cc] = fr[k];
+            }
+            if (lane == 0) {
+                if (accepted) sp_s[i] = static_cast<int8_t>(-si);
+                lg_s[cur - wb] = lg_cur;
+                atomicAdd(&hd[ncur - wb], 1u);
+                act_s[ncur - wb] = 1;
+            }
+            cur = ncur;
+            if (kIT) {
+                lg_cur = stage != kFrozen ? lg_base + factor : lg_base;
+                if (stage == kInverseTime && active_count != 0)
+                    factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + t + 1);
+            } else {
+                lg_cur = frozen ? lg_base : lg_base + factor;
+            }
+
+            __syncwarp();  // the stores are visible to every lane
+            if (lane == 0) st_release_shared(consumed_addr, hq);  // draws before this site are done
+            hq += need_u ? 2u : 1u;
+            i = c;
+            si = s_next;
+            h = h_next;
+            c1 = need_u ? r3 : c2;
+            c2 = need_u ? r4 : r3;
+            lnu = need_u ? l3 : l2;
+            m_prev = m_eff;
+            prev_slot = slot;
+        }
+    };
+    if (!failed) {
+        if (stage == kInverseTime)
+            run(std::true_type{});
+        else
+            run(std::false_type{});
+    }
+    if (!failed) {  // the last attempt's field update
+        const double2* prow2 = reinterpret_cast<const double2*>(ring + static_cast<size_t>(prev_slot) * ld);
 #pragma unroll
         for (int k = 0; k < kChunks; ++k) {
             const int cc = lane + 32 * k;
             if (cc < ld2) {
-                const double2 r = row2[cc];
-                fr[k].x = fma(m_eff, r.x, fr[k].x);
-                fr[k].y = fma(m_eff, r.y, fr[k].y);
-                f2s[cc] = fr[k];
+                const double2 r = prow2[cc];
+                fr[k].x = fma(m_prev, r.x, fr[k].x);
+                fr[k].y = fma(m_prev, r.y, fr[k].y);
             }
         }
-        if (lane == 0 && accepted) sp_s[i] = static_cast<int8_t>(-si);
-        E = accepted ? Ep : E;
-        since = accepted ? 0 : since + 1;
-        n_acc += accepted ? 1u : 0u;
-        n_forced += (accepted && forced) ? 1u : 0u;
-        ++t;
-
-        // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
-        if (stage == kInverseTime) {
-            factor = factor_next;
-            if (factor <= P.final_factor) stage = kFrozen;
-        }
-        const bool move = accepted && nb != cur;
-        if (lane == 0) lg_s[cur - wb] = lg_cur;
-        const int ncur = move ? nb : cur;
-        const double lg_base = move ? lg_new : lg_cur;
-        const uint64_t hv = h_s[ncur - wb];
-        const bool visited = act_s[ncur - wb] != 0;
-        if (lane == 0) h_s[ncur - wb] = hv + 1;
-        if (!visited) {  // rare: first visit of a bin
-            if (lane == 0) act_s[ncur - wb] = 1;
-            ++active_count;
-        }
-        cur = ncur;
-        lg_cur = stage != kFrozen ? lg_base + factor : lg_base;
-        if (stage == kInverseTime && active_count != 0)
-            factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + t + 1);
-
-        // the consumed draws leave the queue; their slots get the draws kQueue ahead
-        const uint64_t d1 = rng.next();
-        Rng r2n = rng;
-        const uint64_t d2 = r2n.next();
-        rng.s0 = need_u ? r2n.s0 : rng.s0;
-        rng.s1 = need_u ? r2n.s1 : rng.s1;
-        rng.s2 = need_u ? r2n.s2 : rng.s2;
-        rng.s3 = need_u ? r2n.s3 : rng.s3;
-        if (lane == 0) {
-            dq[(hq + kQueue) & kQueueMask] = d1;
-            dq[(hq + kQueue + 1) & kQueueMask] = d2;
-        }
-        cp_async_wait<2>();  // the next draw's slot is free to reuse when the uniform was consumed
-        __syncwarp();        // every lane has read the site's row and written its fields
-        copy_row(ring_addr + slot * rs, static_cast<int>(fast_mod(fm, d1)), 16);
-        copy_row(need_u ? ring_addr + ((hq + 1) & (kQueue - 1)) * rs : spare_addr, static_cast<int>(fast_mod(fm, d2)),
-                 need_u ? 16u : 0u);
-        cp_async_commit();
-        hq += need_u ? 2u : 1u;
-        q0 = need_u ? q2 : q1;
-        i = c;
-        si = s_next;
-        h = h_next;
     }
-    cp_async_wait<0>();  // no copy may land after the CTA exits
-    if (lane == 0) lg_s[cur - wb] = lg_cur;
     __syncwarp();
-    for (int k = 0; k < kQueue; ++k) rng_step_back(rng);  // back over the queued draws
+    if (lane == 0) {
+        lg_s[cur - wb] = lg_cur;
+        st_release_shared(consumed_addr, hq);
+        st_release_shared(stop_addr, 1u);
+    }
+    __syncthreads();  // the producer has drained its copies and left its state
+    if (failed || sctl[2] != 0) {
+        if (lane == 0) record_error(ctl, WLG_ERR_TIMEOUT, w);
+        return;
+    }
+    Rng rng{srng[0], srng[1], srng[2], srng[3]};
+    for (uint32_t k = hq; k != sctl[3]; ++k) rng_step_back(rng);  // back over the unconsumed draws
+    // fold the histogram deltas into H; the Wang-Landau count of active bins from the mask
+    uint64_t active_after = 0;
+    for (int b = lane; b < nbins; b += 32) {
+        h_s[b] += hd[b];
+        active_after += act_s[b] ? 1 : 0;
+    }
+    active_after = warp_sum_u64(active_after);
+    if (st.stage != kInverseTime) active_count += active_after - active_before;
+    __syncwarp();
 
     st.rng[0] = rng.s0;
     st.rng[1] = rng.s1;
@@ -765,11 +950,6 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_fast_kernel(EngineView v, W
     }
 }
 
-size_t fast_smem_bytes(const EngineView& v) {
-    return (kQueue + 1) * static_cast<size_t>(v.ld) * 8 + (kQueueMask + 1) * 8 +
-           smem_layout(v.ld, v.max_window_bins, true, false).total;
-}
-
 using SweepFn = void (*)(EngineView, WalkArgs);
 
 template <int P, bool F>
@@ -786,50 +966,55 @@ SweepFn sweep_fn() {
 
 }  // namespace
 
-template <int K>
-SweepFn fast_fn() {
+template <int K, bool kPow2>
+SweepFn split_fn() {
     static bool configured = false;
     if (!configured) {
-        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_dense_fast_kernel<K>),
+        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_dense_split_kernel<K, kPow2>),
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
                    "cudaFuncSetAttribute");
         configured = true;
     }
-    return &sweep_dense_fast_kernel<K>;
+    return &sweep_dense_split_kernel<K, kPow2>;
 }
 
-// The lookahead sweep for FP64 couplings with ld <= 1024 (chunks of 64 doubles per lane pass).
-SweepFn pick_fast(int ld) {
+template <bool kPow2>
+SweepFn pick_split_width(int ld) {
     switch ((ld + 63) / 64) {
-        case 1: return fast_fn<1>();
-        case 2: return fast_fn<2>();
-        case 3: return fast_fn<3>();
-        case 4: return fast_fn<4>();
-        case 5: return fast_fn<5>();
-        case 6: return fast_fn<6>();
-        case 7: return fast_fn<7>();
-        case 8: return fast_fn<8>();
-        case 9: return fast_fn<9>();
-        case 10: return fast_fn<10>();
-        case 11: return fast_fn<11>();
-        case 12: return fast_fn<12>();
-        case 13: return fast_fn<13>();
-        case 14: return fast_fn<14>();
-        case 15: return fast_fn<15>();
-        case 16: return fast_fn<16>();
+        case 1: return split_fn<1, kPow2>();
+        case 2: return split_fn<2, kPow2>();
+        case 3: return split_fn<3, kPow2>();
+        case 4: return split_fn<4, kPow2>();
+        case 5: return split_fn<5, kPow2>();
+        case 6: return split_fn<6, kPow2>();
+        case 7: return split_fn<7, kPow2>();
+        case 8: return split_fn<8, kPow2>();
+        case 9: return split_fn<9, kPow2>();
+        case 10: return split_fn<10, kPow2>();
+        case 11: return split_fn<11, kPow2>();
+        case 12: return split_fn<12, kPow2>();
+        case 13: return split_fn<13, kPow2>();
+        case 14: return split_fn<14, kPow2>();
+        case 15: return split_fn<15, kPow2>();
+        case 16: return split_fn<16, kPow2>();
         default: return nullptr;
     }
+}
+
+// The split sweep for FP64 couplings with ld <= 1024 (chunks of 64 doubles per lane pass).
+SweepFn pick_split(int ld, bool pow2_width) {
+    return pow2_width ? pick_split_width<true>(ld) : pick_split_width<false>(ld);
 }
 
 bool launch_sweep_dense(const EngineView& v, const WalkArgs& a, cudaStream_t stream) {
     const bool features = v.p.collect || v.p.nalivaiko;
     const size_t jbytes = v.precision == WLG_PRECISION_FP64 ? 8 : v.precision == WLG_PRECISION_FP32 ? 4 : 2;
-    if (!features && v.precision == WLG_PRECISION_FP64 && v.ld <= 1024) {  // the lookahead sweep
-        const size_t fast_bytes = fast_smem_bytes(v);
-        SweepFn fn = pick_fast(v.ld);
-        if (fn && fast_bytes <= 227 * 1024) {
-            fn<<<static_cast<unsigned>(a.count), 32, fast_bytes, stream>>>(v, a);
-            check_cuda(cudaGetLastError(), "sweep_dense_fast_kernel");
+    if (!features && v.precision == WLG_PRECISION_FP64 && v.ld <= 1024) {  // the split sweep
+        SweepFn fn = pick_split(v.ld, v.grid.pow2_width != 0);
+        const size_t split_bytes = split_layout(v.ld, v.max_window_bins).total;
+        if (fn && split_bytes <= 227 * 1024) {
+            fn<<<static_cast<unsigned>(a.count), 64, split_bytes, stream>>>(v, a);
+            check_cuda(cudaGetLastError(), "sweep_dense_split_kernel");
             return true;
         }
     }
