@@ -62,7 +62,7 @@ def load_peaks() -> dict:
 
 def ncu_traffic_per_launch():
     """dram bytes per sweep-kernel launch from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / "walk_kernel_dense_rewl_n512.md"
+    p = ROOT / "profiles" / "sweep_dense_split_kernel_rewl_n512.md"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
@@ -253,7 +253,7 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
                                                 "x16 -> wlg_engine_destroy, pinned host buffers"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                         "kernel": "walk_kernel<FP64,dense>", "peak_source": peaks["source"],
+                         "kernel": "sweep_dense_split_kernel<8, pow2 width> (FP64 dense J)", "peak_source": peaks["source"],
                          "bytes_per_launch": bytes_per_launch, "launch_ms": launch_s * 1e3,
                          "acceptance": accepted / max(1, attempted)},
             "gpu_launches": 2 * launches,
