@@ -155,6 +155,21 @@ typedef struct wlg_epoch_timing {
     uint64_t accepted;   /* accepted flips in these epochs, all walkers                  */
 } wlg_epoch_timing;
 
+/* Drift of a mixed-precision run (coupling_precision FP32 or BF16), accumulated over its
+ * periodic FP64 recomputes (recompute_interval_attempts).  No counterpart in the reference,
+ * which stores J in FP64 only. */
+typedef struct wlg_precision_report {
+    int32_t coupling_precision;  /* wlg_precision of the run                                  */
+    int32_t pad;
+    uint64_t recompute_interval_attempts; /* 0: no recompute scheduled                        */
+    uint64_t recomputes;         /* FP64 recompute passes made                                */
+    uint64_t resynced;           /* walker states replaced by the FP64 values                 */
+    uint64_t deferred;           /* resyncs deferred because E64 fell outside the window     */
+    uint64_t bin_changes;        /* resyncs that moved a walker's current bin                 */
+    double max_field_drift;      /* max over recomputes, walkers, sites of |h - h64|          */
+    double max_energy_drift;     /* max over recomputes and walkers of |E - E64|              */
+} wlg_precision_report;
+
 /* wl::WalkerSnapshot (include/wl/wang_landau.hpp:74-89).  The array members point to
  * caller-owned buffers: spins and fields hold n entries, log_g/histogram/active hold
  * grid-bins entries (the whole grid, as in the reference). */
@@ -259,6 +274,9 @@ wlg_status wlg_engine_time_epochs(wlg_engine* engine, uint64_t epochs, wlg_epoch
  * replay (>= 1); 0 leaves a value unchanged.  No counterpart in the reference. */
 wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block,
                                  int32_t epochs_per_graph);
+/* The drift report of a mixed-precision run (all zero for FP64 couplings).  No counterpart
+ * in the reference. */
+wlg_status wlg_engine_precision_report(wlg_engine* engine, wlg_precision_report* out);
 uint64_t wlg_engine_walkers(const wlg_engine* engine);
 uint64_t wlg_engine_bins(const wlg_engine* engine);
 uint64_t wlg_engine_spins(const wlg_engine* engine);

@@ -137,6 +137,20 @@ class wlg_epoch_timing(C.Structure):
     ]
 
 
+class wlg_precision_report(C.Structure):
+    _fields_ = [
+        ("coupling_precision", C.c_int32),
+        ("pad", C.c_int32),
+        ("recompute_interval_attempts", C.c_uint64),
+        ("recomputes", C.c_uint64),
+        ("resynced", C.c_uint64),
+        ("deferred", C.c_uint64),
+        ("bin_changes", C.c_uint64),
+        ("max_field_drift", C.c_double),
+        ("max_energy_drift", C.c_double),
+    ]
+
+
 class wlg_snapshot(C.Structure):
     _fields_ = [
         ("walker_id", C.c_uint64),
@@ -165,6 +179,7 @@ STRUCTS = {
     "wlg_run_totals": wlg_run_totals,
     "wlg_snapshot": wlg_snapshot,
     "wlg_epoch_timing": wlg_epoch_timing,
+    "wlg_precision_report": wlg_precision_report,
 }
 
 P = C.POINTER
@@ -193,6 +208,7 @@ SIGNATURES = {
     "wlg_engine_run_epochs": (_i32, [_vp, _u64, P(_u64), P(_i32)]),
     "wlg_engine_totals": (_i32, [_vp, P(wlg_run_totals)]),
     "wlg_engine_time_epochs": (_i32, [_vp, _u64, P(wlg_epoch_timing)]),
+    "wlg_engine_precision_report": (_i32, [_vp, P(wlg_precision_report)]),
     "wlg_engine_set_launch": (_i32, [_vp, _i32, _i32]),
     "wlg_engine_walkers": (_u64, [_vp]),
     "wlg_engine_bins": (_u64, [_vp]),

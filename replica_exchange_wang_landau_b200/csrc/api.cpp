@@ -338,6 +338,14 @@ wlg_status wlg_engine_time_epochs(wlg_engine* engine, uint64_t epochs, wlg_epoch
     });
 }
 
+wlg_status wlg_engine_precision_report(wlg_engine* engine, wlg_precision_report* out) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] {
+        if (!out) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null output");
+        engine->impl->precision_report(out);
+    });
+}
+
 wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block, int32_t epochs_per_graph) {
     WLG_ENGINE_GUARD(engine)
     return guarded([&] { engine->impl->set_launch(walkers_per_block, epochs_per_graph); });

@@ -255,6 +255,17 @@ struct alignas(16) Control {
     int32_t pad[3];
 };
 
+// Accumulated by the periodic FP64 recompute of a mixed-precision run (precision.cu).
+struct PrecisionReport {
+    unsigned long long max_field_drift_bits;   // max |h - h64| (bits of a non-negative double)
+    unsigned long long max_energy_drift_bits;  // max |E - E64|
+    unsigned long long recomputes;             // recompute passes (host-counted)
+    unsigned long long resynced;               // walker resyncs applied
+    unsigned long long deferred;               // resyncs deferred: E64 outside the window
+    unsigned long long bin_changes;            // resyncs that moved the current bin
+    unsigned long long pad[2];
+};
+
 struct DeviceParams {  // wl::WlParameters + the run_rewl intervals, on the device
     double flatness;
     uint64_t minimum_visits;

@@ -160,6 +160,15 @@ void Engine::initialise_walkers(const wlg_run_config& c) {
     zeroed(d_rep_present_, R);
     zeroed(d_rep_spins_, p_.collect ? R * ld : 16);
     zeroed(d_ctl_, sizeof(Control));
+    zeroed(d_prec_, sizeof(PrecisionReport));
+    if (precision_ != WLG_PRECISION_FP64 && c.recompute_interval_attempts != 0) {
+        // the recompute runs at the first exchange boundary after every interval
+        recompute_epochs_ = std::max<uint64_t>(
+            1, (c.recompute_interval_attempts + c.exchange_interval_attempts - 1) / c.exchange_interval_attempts);
+        next_recompute_ = recompute_epochs_;
+        d_rfields_.allocate(W * ld * sizeof(double));
+        d_renergy_.allocate(W * sizeof(double));
+    }
     d_scratch_.allocate(std::max<size_t>(B * 32 + 256, W * sizeof(wlg_walker_statistics) + 256));
 
     EngineView& v = view_;
@@ -465,9 +474,14 @@ void Engine::run_epochs(uint64_t max_epochs, uint64_t* epochs_run, int32_t* done
             const uint64_t epochs_needed = std::max<uint64_t>(1, (need + p_.exchange_interval - 1) / p_.exchange_interval);
             chunk = std::min(chunk, epochs_needed);
         }
+        if (recompute_epochs_) chunk = std::min(chunk, std::max<uint64_t>(1, next_recompute_ - epochs_));
         launch_epochs(chunk);
         check_device_error();
         budget -= std::min(budget, chunk);
+        if (recompute_epochs_ && !done_ && epochs_ >= next_recompute_) {
+            recompute_fields();
+            next_recompute_ = epochs_ + recompute_epochs_;
+        }
         maybe_checkpoint();
         print_progress(false);
     }
@@ -477,6 +491,32 @@ void Engine::run_epochs(uint64_t max_epochs, uint64_t* epochs_run, int32_t* done
     }
     if (epochs_run) *epochs_run = epochs_ - start;
     if (done) *done = done_ ? 1 : 0;
+}
+
+// The FP64 recompute of a mixed-precision run: all configurations' fields and energies from
+// the FP64 J (reference summation order), then the per-walker drift measurement and resync.
+void Engine::recompute_fields() {
+    compute_fields(view_, d_spins_.get<int8_t>(), static_cast<int64_t>(sys_.ld), d_rfields_.get<double>(),
+                   static_cast<int64_t>(sys_.ld), d_renergy_.get<double>(), static_cast<int>(walkers_), stream_);
+    launch_resync(view_, d_rfields_.get<double>(), d_renergy_.get<double>(), d_prec_.get<PrecisionReport>(),
+                  stream_);
+    ++recomputes_;
+    check_device_error();
+}
+
+void Engine::precision_report(wlg_precision_report* out) {
+    PrecisionReport r{};
+    check_cuda(cudaMemcpyAsync(&r, d_prec_.ptr, sizeof r, cudaMemcpyDeviceToHost, stream_), "copy report");
+    check_cuda(cudaStreamSynchronize(stream_), "sync");
+    *out = wlg_precision_report{};
+    out->coupling_precision = precision_;
+    out->recompute_interval_attempts = recompute_epochs_ ? cfg_.recompute_interval_attempts : 0;
+    out->recomputes = recomputes_;
+    out->resynced = r.resynced;
+    out->deferred = r.deferred;
+    out->bin_changes = r.bin_changes;
+    std::memcpy(&out->max_field_drift, &r.max_field_drift_bits, sizeof(double));
+    std::memcpy(&out->max_energy_drift, &r.max_energy_drift_bits, sizeof(double));
 }
 
 void Engine::run(wlg_run_totals* out) {

@@ -133,6 +133,9 @@ void launch_walk(const EngineView& v, const WalkArgs& a, int walkers_per_block, 
 // sweep.cu: the dense sweep; false when the walker does not fit the shared-memory ring.
 bool launch_sweep_dense(const EngineView& v, const WalkArgs& a, cudaStream_t stream);
 void launch_exchange(const EngineView& v, cudaStream_t stream);
+// precision.cu: drift measurement and resync after an FP64 recompute of all fields.
+void launch_resync(const EngineView& v, const double* rfields, const double* renergy, PrecisionReport* report,
+                   cudaStream_t stream);
 void launch_flush_pending(const EngineView& v, cudaStream_t stream);
 void launch_summarize(const EngineView& v, int window, int allow_empty, double* log_g, uint64_t* hist,
                       double* sem, uint8_t* valid, int* status, cudaStream_t stream);
@@ -174,6 +177,7 @@ class Engine {
     void begin_next_iteration(uint64_t walker);
     double exchange_log_probability(uint64_t left, uint64_t right);
     void swap(uint64_t left, uint64_t right);
+    void precision_report(wlg_precision_report* out);
 
     // Launch shape (chosen by the autotuner or set explicitly).
     int walkers_per_block = 1;
@@ -186,6 +190,7 @@ class Engine {
     void launch_epochs(uint64_t count);
     void build_graph();
     void maybe_checkpoint();
+    void recompute_fields();
     void print_progress(bool final_line);
     std::vector<WalkerState> download_states();
 
@@ -206,6 +211,9 @@ class Engine {
     DeviceBuffer d_win_begin_, d_win_end_, d_ws_, d_log_g_, d_hist_, d_active_, d_refine_, d_sqdisp_,
         d_dsamples_, d_spins_, d_fields_, d_rep_energy_, d_rep_dist_, d_rep_target_, d_rep_present_,
         d_rep_spins_, d_ctl_, d_scratch_;
+    // mixed precision: FP64 recompute every recompute_epochs_ epochs (0 = never)
+    DeviceBuffer d_rfields_, d_renergy_, d_prec_;
+    uint64_t recompute_epochs_ = 0, next_recompute_ = 0, recomputes_ = 0;
     EngineView view_{};
 
     std::string checkpoint_path_;

@@ -305,6 +305,9 @@ class RunConfig:
     checkpoint_path: str = ""
     progress_interval_seconds: float = 0.0
     coupling_precision: str = "fp64"
+    # FP32/BF16 couplings: FP64 recompute of fields and energies every this many MCS (0 = never).
+    # No counterpart in the reference.
+    recompute_interval_mcs: float = 1.0
 
     def resolve_mcs(self, spin_count: int) -> "RunConfig":
         """RunConfig::resolve_mcs (src/io.cpp:210-236)."""
@@ -383,7 +386,8 @@ class RunConfig:
             c.initial_spins_present = _u8ptr(present)
         c.progress_interval_seconds = float(self.progress_interval_seconds)
         c.coupling_precision = _abi.PRECISION[self.coupling_precision]
-        c.recompute_interval_attempts = int(n)
+        c.recompute_interval_attempts = attempts_from_mcs(self.recompute_interval_mcs, n, True,
+                                                          "recompute_interval_mcs")
         return c, keep
 
 
@@ -425,6 +429,7 @@ class RewlResult:
     exchange_accepted: int = 0
     converged: bool = False
     epochs: int = 0
+    precision_report: Optional[dict] = None  # mixed-precision drift (no reference counterpart)
 
 
 @dataclass
@@ -538,6 +543,14 @@ class Engine:
         _check(self._lib.wlg_engine_time_epochs(self._h, int(epochs), C.byref(t)))
         return {name: getattr(t, name) for name, _ in _abi.wlg_epoch_timing._fields_}
 
+    def precision_report(self) -> dict:
+        """Drift of a mixed-precision run over its periodic FP64 recomputes (zeros for FP64)."""
+        r = _abi.wlg_precision_report()
+        _check(self._lib.wlg_engine_precision_report(self._h, C.byref(r)))
+        out = {name: getattr(r, name) for name, _ in _abi.wlg_precision_report._fields_ if name != "pad"}
+        out["coupling_precision"] = {v: k for k, v in _abi.PRECISION.items()}[r.coupling_precision]
+        return out
+
     def set_launch(self, walkers_per_block: int = 0, epochs_per_graph: int = 0) -> None:
         _check(self._lib.wlg_engine_set_launch(self._h, int(walkers_per_block), int(epochs_per_graph)))
 
@@ -588,7 +601,7 @@ class Engine:
         reps = self.representatives() if collect else []
         return RewlResult(fragments, self.walker_statistics(), sampling, reps, t["attempted"], t["accepted"],
                           t["forced_accepted"], t["exchange_attempted"], t["exchange_accepted"], bool(t["converged"]),
-                          t["epochs"])
+                          t["epochs"], self.precision_report())
 
     # single-walker operations (include/wl/wang_landau.hpp:98-138)
     def run_attempts(self, walker: int, count: int) -> None:

@@ -44,6 +44,10 @@ int main(void) {
     F(wlg_run_totals, epochs);
     S(wlg_epoch_timing); F(wlg_epoch_timing, epochs); F(wlg_epoch_timing, walk_ms); F(wlg_epoch_timing, exchange_ms);
     F(wlg_epoch_timing, total_ms); F(wlg_epoch_timing, attempted); F(wlg_epoch_timing, accepted);
+    S(wlg_precision_report); F(wlg_precision_report, coupling_precision); F(wlg_precision_report, pad);
+    F(wlg_precision_report, recompute_interval_attempts); F(wlg_precision_report, recomputes);
+    F(wlg_precision_report, resynced); F(wlg_precision_report, deferred); F(wlg_precision_report, bin_changes);
+    F(wlg_precision_report, max_field_drift); F(wlg_precision_report, max_energy_drift);
     S(wlg_snapshot); F(wlg_snapshot, walker_id); F(wlg_snapshot, spins); F(wlg_snapshot, fields);
     F(wlg_snapshot, energy); F(wlg_snapshot, log_g); F(wlg_snapshot, histogram); F(wlg_snapshot, active);
     F(wlg_snapshot, factor); F(wlg_snapshot, attempted); F(wlg_snapshot, accepted); F(wlg_snapshot, forced_accepted);
