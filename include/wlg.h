@@ -277,6 +277,12 @@ wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block,
 /* The drift report of a mixed-precision run (all zero for FP64 couplings).  No counterpart
  * in the reference. */
 wlg_status wlg_engine_precision_report(wlg_engine* engine, wlg_precision_report* out);
+/* Warm start before the first attempt: every walker's window slice of log g is set from
+ * log_g (grid-bins entries, whole grid; finite inside every window) and its refinement
+ * factor ln f to `factor` (> 0; frozen at once if <= final_factor).  No counterpart in the
+ * reference, whose walkers start from log g = 0 and ln f = 1; the learned warm start
+ * (replica_exchange_wang_landau_b200/warmstart.py) supplies the estimate. */
+wlg_status wlg_engine_warm_start(wlg_engine* engine, const double* log_g, double factor);
 uint64_t wlg_engine_walkers(const wlg_engine* engine);
 uint64_t wlg_engine_bins(const wlg_engine* engine);
 uint64_t wlg_engine_spins(const wlg_engine* engine);
@@ -320,6 +326,33 @@ wlg_status wlg_walker_begin_next_iteration(wlg_engine* engine, uint64_t walker);
 wlg_status wlg_walker_exchange_log_probability(wlg_engine* engine, uint64_t left,
                                                uint64_t right, double* log_probability);
 wlg_status wlg_walker_swap(wlg_engine* engine, uint64_t left, uint64_t right);
+
+/* ---- the warm-start network (no counterpart in the reference) --------------------------
+ * A small multilayer perceptron trained on DOS curves that plain runs produce: inputs are
+ * per-bin features of a system (replica_exchange_wang_landau_b200/warmstart.py), the output
+ * is log g per spin.  Fully connected layers, tanh on hidden layers, identity output, mean
+ * squared error, full-batch Adam; forward, backward and the optimiser run as hand-written
+ * CUDA kernels.  Parameters are FP32 in one array: for each layer l, W_l (dims[l+1] x
+ * dims[l], row-major) then b_l (dims[l+1]).  Host buffers in and out. */
+typedef struct wlg_mlp wlg_mlp;
+/* layers = number of weight layers (1-8); dims has layers+1 widths (1-4096), dims[layers]
+ * = 1.  Glorot-uniform weights from a splitmix64 stream of `seed`, zero biases. */
+wlg_status wlg_mlp_create(int32_t layers, const int32_t* dims, uint64_t seed, wlg_mlp** out);
+void wlg_mlp_destroy(wlg_mlp* mlp);
+uint64_t wlg_mlp_parameter_count(const wlg_mlp* mlp);
+wlg_status wlg_mlp_get_parameters(wlg_mlp* mlp, float* out);
+/* Also resets the optimiser state. */
+wlg_status wlg_mlp_set_parameters(wlg_mlp* mlp, const float* in);
+/* y[batch] = network(x[batch x dims[0]]). */
+wlg_status wlg_mlp_forward(wlg_mlp* mlp, const float* x, uint64_t batch, float* y);
+/* Mean squared error against t[batch] and its gradient with respect to every parameter,
+ * at the current parameters (no update). */
+wlg_status wlg_mlp_gradients(wlg_mlp* mlp, const float* x, const float* t, uint64_t batch, float* grads,
+                             double* loss);
+/* `steps` full-batch Adam steps (beta1 0.9, beta2 0.999, eps 1e-8); *loss = the error after
+ * the last step. */
+wlg_status wlg_mlp_train(wlg_mlp* mlp, const float* x, const float* t, uint64_t batch, uint64_t steps,
+                         double learning_rate, double* loss);
 
 #ifdef __cplusplus
 }

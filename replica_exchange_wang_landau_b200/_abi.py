@@ -209,6 +209,15 @@ SIGNATURES = {
     "wlg_engine_totals": (_i32, [_vp, P(wlg_run_totals)]),
     "wlg_engine_time_epochs": (_i32, [_vp, _u64, P(wlg_epoch_timing)]),
     "wlg_engine_precision_report": (_i32, [_vp, P(wlg_precision_report)]),
+    "wlg_engine_warm_start": (_i32, [_vp, P(_dbl), _dbl]),
+    "wlg_mlp_create": (_i32, [_i32, P(_i32), _u64, P(_vp)]),
+    "wlg_mlp_destroy": (None, [_vp]),
+    "wlg_mlp_parameter_count": (_u64, [_vp]),
+    "wlg_mlp_get_parameters": (_i32, [_vp, P(C.c_float)]),
+    "wlg_mlp_set_parameters": (_i32, [_vp, P(C.c_float)]),
+    "wlg_mlp_forward": (_i32, [_vp, P(C.c_float), _u64, P(C.c_float)]),
+    "wlg_mlp_gradients": (_i32, [_vp, P(C.c_float), P(C.c_float), _u64, P(C.c_float), P(_dbl)]),
+    "wlg_mlp_train": (_i32, [_vp, P(C.c_float), P(C.c_float), _u64, _u64, _dbl, P(_dbl)]),
     "wlg_engine_set_launch": (_i32, [_vp, _i32, _i32]),
     "wlg_engine_walkers": (_u64, [_vp]),
     "wlg_engine_bins": (_u64, [_vp]),

@@ -346,6 +346,11 @@ wlg_status wlg_engine_precision_report(wlg_engine* engine, wlg_precision_report*
     });
 }
 
+wlg_status wlg_engine_warm_start(wlg_engine* engine, const double* log_g, double factor) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] { engine->impl->warm_start(log_g, factor); });
+}
+
 wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block, int32_t epochs_per_graph) {
     WLG_ENGINE_GUARD(engine)
     return guarded([&] { engine->impl->set_launch(walkers_per_block, epochs_per_graph); });
@@ -431,6 +436,72 @@ wlg_status wlg_walker_exchange_log_probability(wlg_engine* engine, uint64_t left
 wlg_status wlg_walker_swap(wlg_engine* engine, uint64_t left, uint64_t right) {
     WLG_ENGINE_GUARD(engine)
     return guarded([&] { engine->impl->swap(left, right); });
+}
+
+}  // extern "C"
+
+// ---- the warm-start network (no counterpart in the reference) ----------------------------
+
+extern "C" {
+
+struct wlg_mlp {
+    wlg::Mlp* impl;
+};
+
+wlg_status wlg_mlp_create(int32_t layers, const int32_t* dims, uint64_t seed, wlg_mlp** out) {
+    return guarded([&] {
+        if (!dims || !out) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        wlg::Mlp* m = wlg::mlp_create(layers, dims, seed);
+        *out = new wlg_mlp{m};
+    });
+}
+
+void wlg_mlp_destroy(wlg_mlp* mlp) {
+    if (!mlp) return;
+    wlg::mlp_destroy(mlp->impl);
+    delete mlp;
+}
+
+uint64_t wlg_mlp_parameter_count(const wlg_mlp* mlp) { return mlp ? wlg::mlp_count(mlp->impl) : 0; }
+
+wlg_status wlg_mlp_get_parameters(wlg_mlp* mlp, float* out) {
+    return guarded([&] {
+        if (!mlp || !out) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        wlg::mlp_get(mlp->impl, out);
+    });
+}
+
+wlg_status wlg_mlp_set_parameters(wlg_mlp* mlp, const float* in) {
+    return guarded([&] {
+        if (!mlp || !in) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        wlg::mlp_set(mlp->impl, in);
+    });
+}
+
+wlg_status wlg_mlp_forward(wlg_mlp* mlp, const float* x, uint64_t batch, float* y) {
+    return guarded([&] {
+        if (!mlp || !x || !y) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        wlg::mlp_forward(mlp->impl, x, batch, y);
+    });
+}
+
+wlg_status wlg_mlp_gradients(wlg_mlp* mlp, const float* x, const float* t, uint64_t batch, float* grads,
+                             double* loss) {
+    return guarded([&] {
+        if (!mlp || !x || !t || !grads || !loss) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        *loss = wlg::mlp_gradients(mlp->impl, x, t, batch, grads);
+    });
+}
+
+wlg_status wlg_mlp_train(wlg_mlp* mlp, const float* x, const float* t, uint64_t batch, uint64_t steps,
+                         double learning_rate, double* loss) {
+    return guarded([&] {
+        if (!mlp || !x || !t || !loss) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        if (!(learning_rate > 0.0) || !std::isfinite(learning_rate))
+            throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "learning rate must be positive");
+        *loss = wlg::mlp_train(mlp->impl, x, t, batch, steps, learning_rate);
+    });
 }
 
 }  // extern "C"

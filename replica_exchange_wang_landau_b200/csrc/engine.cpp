@@ -901,4 +901,35 @@ void Engine::swap(uint64_t left, uint64_t right) {
     if (status) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Replica exchange would violate an energy window");
 }
 
+// Warm start (no counterpart in the reference, whose walkers start from log g = 0 and
+// ln f = 1): before the first attempt, every walker's window slice of log g is set from a
+// whole-grid estimate and its refinement factor to `factor`.  Bins outside the windows stay
+// zero, as in a fresh walker.
+void Engine::warm_start(const double* log_g, double factor) {
+    if (!log_g) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "null log g estimate");
+    if (!std::isfinite(factor) || !(factor > 0.0))
+        throw WlgError(WLG_ERR_INVALID_ARGUMENT, "The warm-start factor must be finite and positive");
+    std::vector<WalkerState> states = download_states();
+    for (const WalkerState& st : states)
+        if (st.attempted != 0) throw WlgError(WLG_ERR_LOGIC, "A warm start must precede the first attempt");
+    for (uint64_t w = 0; w < windows_; ++w)
+        for (uint64_t b = win_[2 * w]; b < win_[2 * w + 1]; ++b)
+            if (!std::isfinite(log_g[b]))
+                throw WlgError(WLG_ERR_INVALID_ARGUMENT, "The log g estimate must be finite inside every window");
+    std::vector<double> grid(walkers_ * bins_, 0.0);
+    for (uint64_t k = 0; k < walkers_; ++k) {
+        const WalkerState& st = states[k];
+        for (uint64_t b = win_[2 * st.window]; b < win_[2 * st.window + 1]; ++b) grid[k * bins_ + b] = log_g[b];
+        states[k].factor = factor;
+        states[k].stage = factor <= p_.final_factor ? kFrozen : kWangLandau;
+    }
+    check_cuda(cudaMemcpyAsync(d_log_g_.ptr, grid.data(), grid.size() * sizeof(double), cudaMemcpyHostToDevice,
+                               stream_),
+               "copy log g");
+    check_cuda(cudaMemcpyAsync(d_ws_.ptr, states.data(), states.size() * sizeof(WalkerState), cudaMemcpyHostToDevice,
+                               stream_),
+               "copy states");
+    check_cuda(cudaStreamSynchronize(stream_), "sync");
+}
+
 }  // namespace wlg

@@ -148,6 +148,17 @@ void launch_begin_next_iteration(const EngineView& v, int walker, int* status, c
 void launch_exchange_pair(const EngineView& v, int left, int right, int do_swap, double* logp, int* status,
                           cudaStream_t stream);
 
+// mlp.cu: the warm-start network (forward, backward and Adam on the device).
+class Mlp;
+Mlp* mlp_create(int layers, const int32_t* dims, uint64_t seed);
+void mlp_destroy(Mlp* m);
+size_t mlp_count(const Mlp* m);
+void mlp_get(Mlp* m, float* out);
+void mlp_set(Mlp* m, const float* in);
+void mlp_forward(Mlp* m, const float* x, uint64_t batch, float* y);
+double mlp_gradients(Mlp* m, const float* x, const float* t, uint64_t batch, float* g);
+double mlp_train(Mlp* m, const float* x, const float* t, uint64_t batch, uint64_t steps, double lr);
+
 // The engine: one REWL run on the current device.
 class Engine {
   public:
@@ -178,6 +189,7 @@ class Engine {
     double exchange_log_probability(uint64_t left, uint64_t right);
     void swap(uint64_t left, uint64_t right);
     void precision_report(wlg_precision_report* out);
+    void warm_start(const double* log_g, double factor);
 
     // Launch shape (chosen by the autotuner or set explicitly).
     int walkers_per_block = 1;

@@ -551,6 +551,14 @@ class Engine:
         out["coupling_precision"] = {v: k for k, v in _abi.PRECISION.items()}[r.coupling_precision]
         return out
 
+    def warm_start(self, log_g: np.ndarray, factor: float) -> None:
+        """Seeds every walker's window slice of log g (whole-grid array) and its ln f before
+        the first attempt (no counterpart in the reference)."""
+        lg = np.ascontiguousarray(log_g, dtype=np.float64)
+        if lg.shape != (self.bins,):
+            raise InvalidArgument(1, "The log g estimate must have one entry per grid bin")
+        _check(self._lib.wlg_engine_warm_start(self._h, _dptr(lg), float(factor)))
+
     def set_launch(self, walkers_per_block: int = 0, epochs_per_graph: int = 0) -> None:
         _check(self._lib.wlg_engine_set_launch(self._h, int(walkers_per_block), int(epochs_per_graph)))
 

@@ -1,0 +1,281 @@
+"""The learned warm start (no counterpart in the reference).
+
+A small MLP, trained on the GPU by the library's own CUDA kernels (csrc/mlp.cu, reached
+through the wlg_mlp_* C-ABI), corrects a physics prior for log g(E) of a dipole system.  It
+is trained on DOS curves that the plain engine produces on generated systems; for a new
+system it predicts log g over the run's grid, and the engine starts its walkers from that
+estimate at a small ln f (Engine.warm_start).  Plain Wang-Landau from a flat start stays the
+fallback: warm_start_or_flat returns the flat start whenever the prediction is unusable, and
+the plain method judges the error of the learned one.
+
+Prior: over uniformly random configurations the energy E = sum_{i<j} J_ij s_i s_j has mean 0,
+variance sigma^2 = sum_{i<j} J_ij^2 and third cumulant tr(J^3), so
+    log g(E) ~ N ln 2 + ln(width) - ln(2 pi sigma^2) / 2 - E^2 / (2 sigma^2)
+per bin of the grid.  The network learns the residual log g - prior from
+    z = E / sigma, emin / sigma, emax / sigma, skewness tr(J^3) / sigma^3, log(N) / log(1024),
+    (E - emin) / (emax - emin), density, nematic order of the easy axes.
+Training curves are normalised so that sum_E g(E) = 2^N over the bins the plain run visited.
+"""
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _abi
+from .engine import Engine, RunConfig, System, WlParameters, _check
+
+FEATURES = 8
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Mlp:
+    """wlg_mlp: tanh MLP with one output; forward, gradients and Adam on the GPU."""
+
+    def __init__(self, dims: Sequence[int], seed: int = 1):
+        self.dims = [int(d) for d in dims]
+        self._lib = _abi.load_library()
+        d = (C.c_int32 * len(self.dims))(*self.dims)
+        h = C.c_void_p()
+        _check(self._lib.wlg_mlp_create(len(self.dims) - 1, d, int(seed), C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.wlg_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def parameter_count(self) -> int:
+        return int(self._lib.wlg_mlp_parameter_count(self._h))
+
+    def parameters(self) -> np.ndarray:
+        out = np.empty(self.parameter_count, np.float32)
+        _check(self._lib.wlg_mlp_get_parameters(self._h, _fptr(out)))
+        return out
+
+    def set_parameters(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.parameter_count:
+            raise ValueError("parameter count mismatch")
+        _check(self._lib.wlg_mlp_set_parameters(self._h, _fptr(p)))
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.empty(x.shape[0], np.float32)
+        _check(self._lib.wlg_mlp_forward(self._h, _fptr(x), x.shape[0], _fptr(y)))
+        return y
+
+    def gradients(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.empty(self.parameter_count, np.float32)
+        loss = C.c_double()
+        _check(self._lib.wlg_mlp_gradients(self._h, _fptr(x), _fptr(t), x.shape[0], _fptr(g), C.byref(loss)))
+        return loss.value, g
+
+    def train(self, x: np.ndarray, t: np.ndarray, steps: int, learning_rate: float) -> float:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = C.c_double()
+        _check(self._lib.wlg_mlp_train(self._h, _fptr(x), _fptr(t), x.shape[0], int(steps), float(learning_rate),
+                                       C.byref(loss)))
+        return loss.value
+
+
+# ---- features and targets ---------------------------------------------------------------
+
+
+def system_descriptor(system: System) -> dict:
+    """Moments of the coupling matrix and geometry descriptors of a dense system."""
+    if system.cutoff > 0.0:
+        raise ValueError("the warm start supports dense systems")
+    g = system.geometry
+    n = g.size()
+    j = np.asarray(system.couplings("fp64"), dtype=np.float64)[:n, :n]
+    sigma = math.sqrt(float(np.sum(np.triu(j, 1) ** 2)))
+    kappa3 = float(np.trace(j @ j @ j))
+    pos = np.asarray(g.positions, dtype=np.float64)
+    box = np.asarray(g.box, dtype=np.float64)
+    extent = np.where(box > 0.0, box, np.ptp(pos, axis=0) + 1.0) if g.periodic else np.ptp(pos, axis=0) + 1.0
+    density = n / float(np.prod(extent))
+    a = np.asarray(g.axes, dtype=np.float64)
+    q = 1.5 * (a.T @ a) / n - 0.5 * np.eye(3)
+    order = float(np.linalg.eigvalsh(q)[-1])
+    return {"n": n, "sigma": sigma, "skew": kappa3 / sigma ** 3 if sigma > 0 else 0.0, "density": density,
+            "order": order}
+
+
+def prior_log_g(desc: dict, emin: float, emax: float, width: float) -> np.ndarray:
+    """The Gaussian prior for log g per bin."""
+    bins = int(round((emax - emin) / width))
+    centre = emin + (np.arange(bins) + 0.5) * width
+    s2 = max(desc["sigma"], 1e-12) ** 2
+    return desc["n"] * math.log(2.0) + math.log(width) - 0.5 * math.log(2 * math.pi * s2) - centre ** 2 / (2 * s2)
+
+
+def bin_features(desc: dict, emin: float, emax: float, width: float) -> np.ndarray:
+    """Feature rows (bins x FEATURES) of one system on one grid."""
+    n = desc["n"]
+    sg = max(desc["sigma"], 1e-12)
+    bins = int(round((emax - emin) / width))
+    centre = emin + (np.arange(bins) + 0.5) * width
+    x = np.empty((bins, FEATURES), np.float64)
+    x[:, 0] = centre / sg
+    x[:, 1] = emin / sg
+    x[:, 2] = emax / sg
+    x[:, 3] = desc["skew"]
+    x[:, 4] = math.log(n) / math.log(1024.0)
+    x[:, 5] = (centre - emin) / (emax - emin)
+    x[:, 6] = desc["density"]
+    x[:, 7] = desc["order"]
+    return x
+
+
+def normalised_log_g(log_g: np.ndarray, valid: np.ndarray, n: int) -> np.ndarray:
+    """log g over the valid bins, shifted so that sum g = 2^N (NaN elsewhere)."""
+    lg = np.asarray(log_g, dtype=np.float64)
+    ok = np.asarray(valid, dtype=bool) & np.isfinite(lg)
+    m = lg[ok].max()
+    lse = m + math.log(np.exp(lg[ok] - m).sum())
+    out = np.full(lg.shape, np.nan)
+    out[ok] = lg[ok] - lse + n * math.log(2.0)
+    return out
+
+
+@dataclass
+class DosSample:
+    """One training curve: a system, its grid and the plain run's log g (with valid bins)."""
+    system: System
+    emin: float
+    emax: float
+    width: float
+    log_g: np.ndarray
+    valid: np.ndarray
+
+
+def plain_dos(system: System, emin: float, emax: float, width: float, seed: int = 1,
+              final_factor: float = 1e-4, walkers: int = 2) -> DosSample:
+    """A DOS curve from the plain engine: one window, flat start, 1/t to final_factor."""
+    c = RunConfig(emin=emin, emax=emax, bin_width=width, windows=1, walkers=walkers, seed=seed)
+    c.wl = WlParameters(0.8, 100, final_factor, 1000, 0, True)
+    c.exchange_interval_mcs = 10.0
+    c.max_mcs = 1e7
+    c.resolve_mcs(system.size())
+    with Engine(system, c) as e:
+        e.run()
+        frag = e.fragment(0, allow_empty=True)
+    return DosSample(system, emin, emax, width, np.asarray(frag.log_g, np.float64), np.asarray(frag.valid, bool))
+
+
+@dataclass
+class WarmStartModel:
+    """Feature and target scalings plus the trained network."""
+    hidden: tuple = (32, 32)
+    seed: int = 1
+    x_mean: Optional[np.ndarray] = None
+    x_std: Optional[np.ndarray] = None
+    t_mean: float = 0.0
+    t_std: float = 1.0
+    net: Optional[Mlp] = field(default=None, repr=False)
+    final_loss: float = math.nan
+
+    def dataset(self, samples: Sequence[DosSample]):
+        xs, ts = [], []
+        for s in samples:
+            desc = system_descriptor(s.system)
+            x = bin_features(desc, s.emin, s.emax, s.width)
+            t = normalised_log_g(s.log_g, s.valid, desc["n"]) - prior_log_g(desc, s.emin, s.emax, s.width)
+            ok = np.isfinite(t)
+            xs.append(x[ok])
+            ts.append(t[ok])
+        return np.concatenate(xs), np.concatenate(ts)
+
+    def fit(self, samples: Sequence[DosSample], steps: int = 4000, learning_rate: float = 3e-3) -> float:
+        x, t = self.dataset(samples)
+        self.x_mean = x.mean(axis=0)
+        self.x_std = np.maximum(x.std(axis=0), 1e-6)
+        self.t_mean = float(t.mean())
+        self.t_std = max(float(t.std()), 1e-6)
+        xn = (x - self.x_mean) / self.x_std
+        tn = (t - self.t_mean) / self.t_std
+        self.net = Mlp([FEATURES, *self.hidden, 1], seed=self.seed)
+        self.final_loss = self.net.train(xn, tn, steps, learning_rate)
+        return self.final_loss
+
+    def predict_log_g(self, system: System, emin: float, emax: float, width: float) -> np.ndarray:
+        """Predicted log g over every bin of the grid (normalised so that sum g = 2^N)."""
+        if self.net is None:
+            raise RuntimeError("the warm-start model is not trained")
+        desc = system_descriptor(system)
+        x = (bin_features(desc, emin, emax, width) - self.x_mean) / self.x_std
+        residual = self.net.forward(x).astype(np.float64) * self.t_std + self.t_mean
+        return prior_log_g(desc, emin, emax, width) + residual
+
+
+def warm_start_or_flat(engine: Engine, model: Optional[WarmStartModel], system: System, emin: float, emax: float,
+                       width: float, factor: float) -> bool:
+    """Starts the engine's walkers from the model's log g at ln f = factor; falls back to the
+    plain flat start (and returns False) when there is no model or the prediction is not
+    finite."""
+    if model is None or model.net is None:
+        return False
+    lg = model.predict_log_g(system, emin, emax, width)
+    if not np.all(np.isfinite(lg)):
+        return False
+    engine.warm_start(lg - lg.max(), factor)
+    return True
+
+
+def run_to_accuracy(system: System, emin: float, emax: float, width: float, reference_log_g: np.ndarray,
+                    tolerance: float, seed: int, model: Optional[WarmStartModel] = None, factor: float = 1e-2,
+                    final_factor: float = 1e-6, walkers: int = 2, chunk_epochs: int = 20,
+                    max_attempts: int = 200_000_000) -> dict:
+    """Time to a given accuracy: one window, 1/t Wang-Landau, flat start (model None) or the
+    model's warm start at ln f = factor; every chunk_epochs epochs the merged log g is compared
+    with reference_log_g (finite on the reference's occupied bins) as max |d - mean(d)| over
+    those bins once all of them are valid.  Returns the attempts per walker and the seconds of
+    the run loop until the tolerance was met (None if it never was), and the final error."""
+    import time
+
+    c = RunConfig(emin=emin, emax=emax, bin_width=width, windows=1, walkers=walkers, seed=seed)
+    c.wl = WlParameters(0.8, 100, final_factor, 1000, 0, True)
+    c.exchange_interval_mcs = 10.0
+    c.max_mcs = 1e12
+    c.resolve_mcs(system.size())
+    ref = np.asarray(reference_log_g, dtype=np.float64)
+    occ = np.isfinite(ref)
+
+    def error(e: Engine) -> float:
+        frag = e.fragment(0, allow_empty=True)
+        if not np.all(frag.valid[occ] == 1):
+            return math.inf
+        d = frag.log_g[occ] - ref[occ]
+        return float(np.max(np.abs(d - d.mean())))
+
+    with Engine(system, c) as e:
+        warm = warm_start_or_flat(e, model, system, emin, emax, width, factor)
+        t0 = time.perf_counter()
+        hit_attempts = hit_seconds = None
+        err = math.inf
+        while True:
+            e.run_epochs(chunk_epochs)
+            t = e.totals()
+            err = error(e)
+            per_walker = t["attempted"] // walkers
+            if err <= tolerance:
+                hit_attempts, hit_seconds = per_walker, time.perf_counter() - t0
+                break
+            if t["converged"] or per_walker >= max_attempts:
+                break
+    return {"warm": warm, "attempts": hit_attempts, "seconds": hit_seconds, "final_error": err}
