@@ -139,23 +139,30 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
     eng = E.Engine(system, config)
     epochs = args.epochs_per_step
     for _ in range(args.warmup):
-        eng.time_epochs(epochs)
+        eng.time_run(epochs)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    walk_ms = exch_ms = total_ms = 0.0
+    total_ms = 0.0
     attempted = accepted = 0
     with ClockSampler(local) as clocks:
         for _ in range(args.steps):
             flush_l2(torch, flush)
             torch.cuda.synchronize()
-            t = eng.time_epochs(epochs)
-            walk_ms += t["walk_ms"]
-            exch_ms += t["exchange_ms"]
+            # the product path: run_epochs (CUDA-graph replays of [sweep, exchange]) with one
+            # CUDA event before and one after on the engine's stream
+            t = eng.time_run(epochs)
             total_ms += t["total_ms"]
             attempted += t["attempted"]
             accepted += t["accepted"]
         torch.cuda.synchronize()
+    # per-kernel device times for the roofline: the same epochs launched one kernel at a
+    # time with CUDA events around every launch (after the timed region)
+    kernel_epochs = min(epochs, 50)
+    flush_l2(torch, flush)
+    torch.cuda.synchronize()
+    kt = eng.time_epochs(kernel_epochs)
+    walk_ms, exch_ms = kt["walk_ms"], kt["exchange_ms"]
     if dist:
         dist.barrier()
     clock = clocks.summary()
@@ -171,7 +178,7 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
         total_max, walk_max, att_all, acc_all = total_ms, walk_ms, attempted, accepted
     value = att_all / (total_max / 1e3)
 
-    # graph-replay throughput of the product path (run_epochs), same workload, for context
+    # host wall-clock throughput of the same path (run_epochs), for context
     torch.cuda.synchronize()
     g0 = time.perf_counter()
     before = eng.totals()["attempted"]
@@ -230,8 +237,9 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
     # accepted flip (fields, spins and the window's log_g/H live in shared memory)
     peaks = load_peaks()
     launches = args.steps * epochs
-    bytes_per_launch = accepted * n * 8 / launches
-    launch_s = (walk_ms / launches) / 1e3
+    k_launches = max(1, kt["epochs"])
+    bytes_per_launch = kt["accepted"] * n * 8 / k_launches
+    launch_s = (walk_ms / k_launches) / 1e3
     achieved = bytes_per_launch / launch_s / 1e9
     traffic = ncu_traffic_per_launch()
 
@@ -255,15 +263,107 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
                          "kernel": "sweep_dense_split_kernel<8, pow2 width> (FP64 dense J)", "peak_source": peaks["source"],
                          "bytes_per_launch": bytes_per_launch, "launch_ms": launch_s * 1e3,
-                         "acceptance": accepted / max(1, attempted)},
+                         "acceptance": kt["accepted"] / max(1, kt["attempted"]),
+                         "kernel_timing": f"{k_launches} epochs launched one kernel at a time with CUDA events "
+                                          f"around each launch, after the timed region"},
             "gpu_launches": 2 * launches,
-            "graph_replay_attempts_per_s": graph_rate,
+            "wall_clock_attempts_per_s": graph_rate,
             "clocks": clock,
-            "exchange_ms_per_step": exch_ms / args.steps,
+            "exchange_ms_per_epoch": exch_ms / k_launches,
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if world == 1 and not args.skip_extras:
+            try:
+                line["mixed_precision"] = mixed_precision_lines(min(epochs, 30))
+            except Exception as exc:  # reported, never fatal to the headline line
+                line["mixed_precision"] = {"error": str(exc)}
+            try:
+                line["time_to_accuracy"] = time_to_accuracy()
+            except Exception as exc:
+                line["time_to_accuracy"] = {"error": str(exc)}
         print(json.dumps(line))
+
+
+def mixed_precision_lines(epochs: int) -> dict:
+    """The same workload with FP32 and BF16 (+ row scale) couplings: device attempts/s of the
+    sweeps and the drift that the periodic FP64 recompute (every 10 MCS) measured."""
+    from replica_exchange_wang_landau_b200.engine import Engine
+    out = {}
+    for precision in ("fp32", "bf16"):
+        system, config = make_workload(seed=1)
+        config.coupling_precision = precision
+        config.recompute_interval_mcs = 10.0
+        with Engine(system, config) as eng:
+            eng.run_epochs(3)
+            t = eng.time_epochs(epochs)
+            eng.run_epochs(epochs)
+            rep = eng.precision_report()
+        out[precision] = {"value": t["attempted"] / (t["total_ms"] / 1e3), "unit": UNIT,
+                          "epochs_timed": t["epochs"], "recompute_interval_mcs": 10.0,
+                          "recomputes": rep["recomputes"], "max_field_drift": rep["max_field_drift"],
+                          "max_energy_drift": rep["max_energy_drift"], "deferred": rep["deferred"],
+                          "bin_changes": rep["bin_changes"]}
+    return out
+
+
+def _cluster(k: int):
+    from replica_exchange_wang_landau_b200.engine import System
+    from replica_exchange_wang_landau_b200.geometry import random_sequential
+    rng = np.random.default_rng(k)
+    n = int(rng.integers(8, 13))
+    return System(random_sequential(n, float(rng.uniform(0.3, 0.8)), 0.8, seed=k), 1.0, 0.0)
+
+
+def _enumerate(system):
+    """Exact log g of a small system by enumerating its 2^N configurations (numpy), on a grid
+    of about 64 power-of-two bins padded by one bin."""
+    import itertools
+    import math
+    n = system.size()
+    j = system.couplings("fp64")[:n, :n]
+    states = np.array(list(itertools.product([-1.0, 1.0], repeat=n)))
+    e = 0.5 * np.einsum("ki,ij,kj->k", states, j, states)
+    w = 2.0 ** round(math.log2((e.max() - e.min()) / 64))
+    emin, emax = math.floor(e.min() / w) * w - w, math.ceil(e.max() / w) * w + w
+    counts = np.bincount(np.floor((e - emin) / w).astype(int), minlength=int(round((emax - emin) / w)))
+    ref = np.where(counts > 0, np.log(np.maximum(counts, 1).astype(float)), np.nan)
+    return emin, emax, w, ref
+
+
+def time_to_accuracy(tolerance: float = 0.05) -> dict:
+    """Learned vs plain: the warm-start network is trained on the GPU on 48 plain-run DOS
+    curves of random dipole clusters (8-12 spins, density 0.3-0.8, random axes); each of 6
+    held-out clusters is then run from the flat start and from the learned start (ln f =
+    1e-2) until max |d log g| against exact enumeration is <= tolerance."""
+    from replica_exchange_wang_landau_b200.warmstart import WarmStartModel, plain_dos, run_to_accuracy
+    t0 = time.perf_counter()
+    train = []
+    for k in range(1, 49):
+        s = _cluster(k)
+        emin, emax, w, _ = _enumerate(s)
+        train.append(plain_dos(s, emin, emax, w, seed=k, final_factor=1e-4))
+    model = WarmStartModel(hidden=(32, 32), seed=3)
+    loss = model.fit(train, steps=4000, learning_rate=3e-3)
+    train_s = time.perf_counter() - t0
+    rows = []
+    for k in range(101, 107):
+        s = _cluster(k)
+        emin, emax, w, ref = _enumerate(s)
+        a = run_to_accuracy(s, emin, emax, w, ref, tolerance, seed=k)
+        b = run_to_accuracy(s, emin, emax, w, ref, tolerance, seed=k, model=model, factor=1e-2)
+        rows.append({"spins": s.size(), "plain_attempts": a["attempts"], "plain_s": a["seconds"],
+                     "learned_attempts": b["attempts"], "learned_s": b["seconds"]})
+    ok = [r for r in rows if r["plain_attempts"] and r["learned_attempts"]]
+    pa = sum(r["plain_attempts"] for r in ok)
+    la = sum(r["learned_attempts"] for r in ok)
+    ps = sum(r["plain_s"] for r in ok)
+    ls = sum(r["learned_s"] for r in ok)
+    return {"tolerance": tolerance, "criterion": "max |d log g| vs exact enumeration, 1 window x 2 walkers, 1/t",
+            "training": {"curves": len(train), "final_loss": loss, "seconds": train_s},
+            "held_out": rows, "plain_attempts_per_walker": pa, "learned_attempts_per_walker": la,
+            "plain_seconds": ps, "learned_seconds": ls, "attempts_ratio": la / pa if pa else None,
+            "seconds_ratio": ls / ps if ps else None}
 
 
 def reference_rate(mcs: float, threads: int, seed: int = 1):
@@ -330,6 +430,8 @@ def main() -> None:
     ap.add_argument("--cpu-sample-mcs", type=float, default=400.0)
     ap.add_argument("--reference-step-mcs", type=float, default=50.0)
     ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--skip-extras", action="store_true",
+                    help="skip the mixed-precision lines and the learned-vs-plain time to accuracy")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -270,6 +270,10 @@ wlg_status wlg_engine_totals(wlg_engine* engine, wlg_run_totals* totals);
 /* The same epochs as wlg_engine_run_epochs, launched one kernel at a time with CUDA events
  * around each kernel on the engine's stream (profiling; no counterpart in the reference). */
 wlg_status wlg_engine_time_epochs(wlg_engine* engine, uint64_t epochs, wlg_epoch_timing* out);
+/* The same epochs as wlg_engine_run_epochs (CUDA-graph replays), with one CUDA event before
+ * and one after on the engine's stream: total_ms is the device time of the whole product
+ * path; walk_ms and exchange_ms are 0.  No counterpart in the reference. */
+wlg_status wlg_engine_time_run(wlg_engine* engine, uint64_t epochs, wlg_epoch_timing* out);
 /* Launch shape: walkers per CTA of the sweep kernel (1-8) and epochs per CUDA-graph
  * replay (>= 1); 0 leaves a value unchanged.  No counterpart in the reference. */
 wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block,

@@ -338,6 +338,14 @@ wlg_status wlg_engine_time_epochs(wlg_engine* engine, uint64_t epochs, wlg_epoch
     });
 }
 
+wlg_status wlg_engine_time_run(wlg_engine* engine, uint64_t epochs, wlg_epoch_timing* out) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] {
+        if (!out) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null output");
+        engine->impl->time_run(epochs, out);
+    });
+}
+
 wlg_status wlg_engine_precision_report(wlg_engine* engine, wlg_precision_report* out) {
     WLG_ENGINE_GUARD(engine)
     return guarded([&] {

@@ -5,11 +5,13 @@
 // of [walk_kernel -> exchange_kernel] pairs captured once in a CUDA graph and replayed; the
 // device keeps the epoch counter and the termination flag, so a replay after termination is
 // a sequence of no-op launches and the host only reads the control block between replays.
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <iostream>
 #include <limits>
+#include <mutex>
 #include <sstream>
 
 #include "engine.hpp"
@@ -36,19 +38,43 @@ bool parameters_valid(const wlg_wl_parameters& p) {
            !(p.round_trip_margin_fraction >= 0.5);
 }
 
+// The device check, once per device (cudaGetDeviceProperties alone took 8-60 ms per call).
 void require_device() {
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
         throw WlgError(WLG_ERR_DEVICE, "No CUDA device is available; this engine runs on an sm_100 (B200) GPU only");
     int device = 0;
     check_cuda(cudaGetDevice(&device), "cudaGetDevice");
-    cudaDeviceProp prop{};
-    check_cuda(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
-    if (prop.major != 10)
+    static std::atomic<uint64_t> checked{0};
+    if (device < 64 && (checked.load() >> device & 1)) return;
+    int major = 0;
+    check_cuda(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device), "cudaDeviceGetAttribute");
+    if (major != 10) {
+        cudaDeviceProp prop{};
+        check_cuda(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
         throw WlgError(WLG_ERR_DEVICE, std::string("This engine is built for sm_100a (B200); found ") + prop.name);
+    }
+    if (device < 64) checked.fetch_or(uint64_t{1} << device);
 }
 
 }  // namespace
+
+cudaStream_t pool_stream() {
+    static std::mutex mu;
+    static cudaStream_t streams[64] = {};
+    int device = 0;
+    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    if (device >= 64) throw WlgError(WLG_ERR_DEVICE, "device index beyond 63");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!streams[device]) {
+        cudaMemPool_t pool = nullptr;
+        check_cuda(cudaDeviceGetDefaultMemPool(&pool, device), "cudaDeviceGetDefaultMemPool");
+        uint64_t keep = ~0ULL;
+        check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
+        check_cuda(cudaStreamCreateWithFlags(&streams[device], cudaStreamNonBlocking), "cudaStreamCreate");
+    }
+    return streams[device];
+}
 
 Engine::Engine(const wlg_system& system, const wlg_run_config& c) : cfg_(c) {
     // RunConfig::validate (src/io.cpp:243-268), as run_rewl calls it.
@@ -522,6 +548,37 @@ void Engine::precision_report(wlg_precision_report* out) {
 void Engine::run(wlg_run_totals* out) {
     while (!done_) run_epochs(~0ULL, nullptr, nullptr);
     if (out) totals(out);
+}
+
+// The product path (run_epochs: CUDA-graph replays and the host's checks between them) with
+// one CUDA event before and one after, on the engine's stream.
+void Engine::time_run(uint64_t epochs, wlg_epoch_timing* out) {
+    wlg_run_totals before{}, after{};
+    totals(&before);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    check_cuda(cudaEventCreate(&e0), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&e1), "cudaEventCreate");
+    try {
+        const uint64_t start = epochs_;
+        check_cuda(cudaEventRecord(e0, stream_), "record");
+        run_epochs(epochs, nullptr, nullptr);
+        check_cuda(cudaEventRecord(e1, stream_), "record");
+        check_cuda(cudaEventSynchronize(e1), "sync");
+        float ms = 0.f;
+        check_cuda(cudaEventElapsedTime(&ms, e0, e1), "elapsed");
+        totals(&after);
+        *out = wlg_epoch_timing{};
+        out->epochs = epochs_ - start;
+        out->total_ms = ms;
+        out->attempted = after.attempted - before.attempted;
+        out->accepted = after.accepted - before.accepted;
+    } catch (...) {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
 }
 
 void Engine::time_epochs(uint64_t epochs, wlg_epoch_timing* out) {

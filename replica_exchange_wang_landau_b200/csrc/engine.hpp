@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <exception>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -25,24 +26,45 @@ inline void check_cuda(cudaError_t e, const char* what) {
         throw WlgError(WLG_ERR_DEVICE, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
 }
 
-// Owning device allocation.
+// The stream on which the current device's buffers are allocated and freed from its default
+// memory pool.  Created once per device and kept; the pool keeps freed memory (release
+// threshold = unlimited) so that creating and destroying engines costs no driver-level
+// allocation after the first one.  (cudaMalloc / cudaFree took up to hundreds of ms per
+// engine destruction.)
+cudaStream_t pool_stream();
+
+// Owning device allocation, stream-ordered on pool_stream().  The allocation is complete
+// before allocate() returns, so any stream may use it.  The owner must have finished every
+// use of the buffer when it is released (the engine and the helpers synchronise their stream
+// first); while an exception unwinds, release() synchronises the device before freeing, so a
+// kernel left in flight by the error cannot write into reused memory.
 struct DeviceBuffer {
     void* ptr = nullptr;
     size_t bytes = 0;
+    cudaStream_t stream = nullptr;
     DeviceBuffer() = default;
     explicit DeviceBuffer(size_t b) { allocate(b); }
     DeviceBuffer(const DeviceBuffer&) = delete;
     DeviceBuffer& operator=(const DeviceBuffer&) = delete;
-    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes) { o.ptr = nullptr; o.bytes = 0; }
+    DeviceBuffer(DeviceBuffer&& o) noexcept : ptr(o.ptr), bytes(o.bytes), stream(o.stream) {
+        o.ptr = nullptr;
+        o.bytes = 0;
+    }
     ~DeviceBuffer() { release(); }
     void allocate(size_t b) {
         release();
         if (b == 0) b = 16;
-        check_cuda(cudaMalloc(&ptr, b), "cudaMalloc");
+        cudaStream_t s = pool_stream();
+        check_cuda(cudaMallocAsync(&ptr, b, s), "cudaMallocAsync");
+        stream = s;
         bytes = b;
+        check_cuda(cudaStreamSynchronize(s), "allocation");
     }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) {
+            if (std::uncaught_exceptions() > 0) cudaDeviceSynchronize();
+            cudaFreeAsync(ptr, stream);
+        }
         ptr = nullptr;
         bytes = 0;
     }
@@ -171,6 +193,7 @@ class Engine {
     void run_epochs(uint64_t max_epochs, uint64_t* epochs_run, int32_t* done);
     void totals(wlg_run_totals* out);
     void time_epochs(uint64_t epochs, wlg_epoch_timing* out);
+    void time_run(uint64_t epochs, wlg_epoch_timing* out);
     void set_launch(int walkers_per_block, int epochs_per_graph);
     uint64_t walkers() const { return walkers_; }
     uint64_t bins() const { return bins_; }

@@ -1,10 +1,10 @@
 // noalloc.cu — local fields and energies without any device allocation.
 //
 // wlg_local_fields builds the coupling matrix and stages spins, fields and energies in
-// buffers it allocates with cudaMalloc.  Some callers cannot allow that: a host that has
-// already handed nearly all device memory to its own pool (a caching allocator reserves it
-// up front), code that must not add the implicit device synchronisation cudaMalloc/cudaFree
-// can cause, or a plugin host that forbids allocation once it has started.  For them this
+// device buffers it allocates (from the device's memory pool).  Some callers cannot allow
+// that: a host that has already handed nearly all device memory to its own pool (a caching
+// allocator reserves it up front), code that must not add the synchronisation a device
+// allocation can cause, or a plugin host that forbids allocation once it has started.  For them this
 // file keeps every intermediate in one statically sized device array instead.
 //
 // The array is a file-scope __device__ object, so every GPU that loads the library holds

@@ -543,6 +543,13 @@ class Engine:
         _check(self._lib.wlg_engine_time_epochs(self._h, int(epochs), C.byref(t)))
         return {name: getattr(t, name) for name, _ in _abi.wlg_epoch_timing._fields_}
 
+    def time_run(self, epochs: int) -> dict:
+        """Runs `epochs` epochs through the product path (graph replays) with CUDA events
+        around the whole run (device time, ms)."""
+        t = _abi.wlg_epoch_timing()
+        _check(self._lib.wlg_engine_time_run(self._h, int(epochs), C.byref(t)))
+        return {name: getattr(t, name) for name, _ in _abi.wlg_epoch_timing._fields_}
+
     def precision_report(self) -> dict:
         """Drift of a mixed-precision run over its periodic FP64 recomputes (zeros for FP64)."""
         r = _abi.wlg_precision_report()
