@@ -495,15 +495,16 @@ constexpr int kDrawBatch = 4;  // draws per producer batch (one barrier per batc
 constexpr int kRingLog = 4;
 
 struct SplitLayout {
-    size_t ring, bars, lnu, site, hd, ctl, base, total;
+    size_t ring, bars, lnu, rs, site, hd, ctl, base, total;
 };
-__host__ __device__ inline SplitLayout split_layout(int ld, int mwb) {
+__host__ __device__ inline SplitLayout split_layout(int ld, int mwb, size_t jbytes) {
     constexpr size_t q = size_t{1} << kRingLog;
     SplitLayout L;
     size_t at = 0;
-    L.ring = at; at += q * static_cast<size_t>(ld) * 8;
+    L.ring = at; at += q * round16(static_cast<size_t>(ld) * jbytes);
     L.bars = at; at += round16((q / kDrawBatch) * 8);
     L.lnu = at; at += round16(q * 8);
+    L.rs = at; at += round16(q * 8);  // BF16: the row scale of each draw's site
     L.site = at; at += round16(q * 4);
     L.hd = at; at += round16(static_cast<size_t>(mwb) * 4);
     L.ctl = at; at += 64;  // consumed, stop, producer status, produced, rng[4]
@@ -527,8 +528,29 @@ __device__ __forceinline__ bool mbar_wait_thread(uint32_t bar, uint32_t parity) 
     return false;
 }
 
-template <int kChunks, bool kPow2>
+// One coupling of a row in shared memory, and the pair (2c, 2c+1), as exact doubles.
+template <int kPrec>
+__device__ __forceinline__ double coupling(const typename CouplingType<kPrec>::T* row, int j) {
+    if constexpr (kPrec == WLG_PRECISION_FP64) return row[j];
+    else if constexpr (kPrec == WLG_PRECISION_FP32) return static_cast<double>(row[j]);
+    else return static_cast<double>(__bfloat162float(row[j]));
+}
+template <int kPrec>
+__device__ __forceinline__ double2 coupling_pair(const typename CouplingType<kPrec>::T* row, int c) {
+    if constexpr (kPrec == WLG_PRECISION_FP64) {
+        return reinterpret_cast<const double2*>(row)[c];
+    } else if constexpr (kPrec == WLG_PRECISION_FP32) {
+        const float2 f = reinterpret_cast<const float2*>(row)[c];
+        return make_double2(f.x, f.y);
+    } else {
+        const __nv_bfloat162 b = reinterpret_cast<const __nv_bfloat162*>(row)[c];
+        return make_double2(__bfloat162float(b.x), __bfloat162float(b.y));
+    }
+}
+
+template <int kChunks, bool kPow2, int kPrec>
 __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, WalkArgs a) {
+    using JT = typename CouplingType<kPrec>::T;
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr int qlog = kRingLog;
     constexpr uint32_t qm = (1u << qlog) - 1u;
@@ -541,10 +563,12 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
     if (a.epoch_mode && *reinterpret_cast<volatile int32_t*>(&ctl->done)) return;
 
     const int ld = v.ld;
-    const SplitLayout SL = split_layout(ld, v.max_window_bins);
+    const SplitLayout SL = split_layout(ld, v.max_window_bins, sizeof(JT));
     const SmemLayout L = smem_layout(ld, v.max_window_bins, true, false);
-    const double* ring = reinterpret_cast<const double*>(smem + SL.ring);
+    const size_t row_stride = round16(static_cast<size_t>(ld) * sizeof(JT)) / sizeof(JT);  // elements
+    const JT* ring = reinterpret_cast<const JT*>(smem + SL.ring);
     double* rec_lnu = reinterpret_cast<double*>(smem + SL.lnu);
+    double* rec_rs = reinterpret_cast<double*>(smem + SL.rs);
     int32_t* rec_site = reinterpret_cast<int32_t*>(smem + SL.site);
     uint32_t* hd = reinterpret_cast<uint32_t*>(smem + SL.hd);
     uint32_t* sctl = reinterpret_cast<uint32_t*>(smem + SL.ctl);  // [0] consumed [1] stop [2] status [3] produced
@@ -558,7 +582,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
     const uint32_t ring_addr = smem_addr(smem + SL.ring);
     const uint32_t bar_addr = smem_addr(smem + SL.bars);
     const uint32_t consumed_addr = smem_addr(sctl), stop_addr = consumed_addr + 4;
-    const uint32_t row_bytes = static_cast<uint32_t>(ld) * 8u;
+    const uint32_t row_bytes = static_cast<uint32_t>(row_stride * sizeof(JT));
 
     WalkerState st = v.ws[w];
     const int wb = v.win_begin[st.window], we = v.win_end[st.window], nbins = we - wb;
@@ -615,7 +639,9 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
     if (warp == 1) {
         // ---- producer: batches of kDrawBatch draws, lane j < kDrawBatch handles draw j ----
         const FastMod fm = v.site_mod;
-        const double* J = v.J64;
+        const JT* J = kPrec == WLG_PRECISION_FP64   ? reinterpret_cast<const JT*>(v.J64)
+                      : kPrec == WLG_PRECISION_FP32 ? reinterpret_cast<const JT*>(v.J32)
+                                                    : reinterpret_cast<const JT*>(v.J16);
         Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};
         uint32_t produced = 0, status = 0;
         for (;;) {
@@ -649,6 +675,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
                 site = mine < fm.threshold ? -1 : static_cast<int>(fast_mod(fm, mine));
                 rec_lnu[e] = log(fmax(to_uniform(mine), 0x1.0p-53));
                 rec_site[e] = site;
+                if constexpr (kPrec == WLG_PRECISION_BF16) rec_rs[e] = static_cast<double>(v.Jscale[site < 0 ? 0 : site]);
             }
             const uint32_t n = produced >> 2;  // batch index
             const uint32_t bar = bar_addr + 8 * (n & bm);
@@ -659,7 +686,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
                              : "memory");
             __syncwarp();
             if (lane < kDrawBatch) {
-                const double* src = J + static_cast<size_t>(site < 0 ? 0 : site) * ld;
+                const JT* src = J + static_cast<size_t>(site < 0 ? 0 : site) * ld;
                 asm volatile(
                     "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                         ring_addr + e * row_bytes),
@@ -727,7 +754,8 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
         }
     }
     // The field update of an attempt is applied during the next one: m_prev and prev_slot
-    // are its factor and row.  Shared memory holds the fields up to the attempt before.
+    // are its factor (times the row scale for BF16) and row.  Shared memory holds the
+    // fields up to the attempt before.
     double m_prev = 0.0;
     uint32_t prev_slot = 0;
     uint64_t active_before = 0;
@@ -748,13 +776,13 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
                 failed = true;
                 break;
             }
-            const double* prow = ring + static_cast<size_t>(prev_slot) * ld;
+            const JT* prow = ring + static_cast<size_t>(prev_slot) * row_stride;
             if (i < 0) {  // rare: bounded() rejects draw hq; the next draw is the candidate site
                 hq += 1;
                 i = c1;
                 if (i >= 0) {
                     si = sp_s[i];
-                    h = fma(m_prev, prow[i], f_s[i]);
+                    h = fma(m_prev, coupling<kPrec>(prow, i), f_s[i]);
                 }
                 c1 = c2;
                 c2 = rec_site[(hq + 2) & qm];
@@ -762,7 +790,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
                 continue;
             }
             const uint32_t slot = hq & qm;
-            const double* row = ring + static_cast<size_t>(slot) * ld;
+            const JT* row = ring + static_cast<size_t>(slot) * row_stride;
             // loads: the next attempt's records, the candidates' fields, spins and couplings,
             // the previous attempt's row
             const int r3 = rec_site[(hq + 3) & qm], r4 = rec_site[(hq + 4) & qm];
@@ -770,14 +798,14 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
             const int c1l = c1 < 0 ? 0 : c1, c2l = c2 < 0 ? 0 : c2;
             const double f1 = f_s[c1l], f2 = f_s[c2l];
             const int s1 = sp_s[c1l], s2 = sp_s[c2l];
-            const double r1 = row[c1l], r2 = row[c2l];
-            const double p1 = prow[c1l], p2 = prow[c2l];
-            const double2* prow2 = reinterpret_cast<const double2*>(prow);
+            const double r1 = coupling<kPrec>(row, c1l), r2 = coupling<kPrec>(row, c2l);
+            const double p1 = coupling<kPrec>(prow, c1l), p2 = coupling<kPrec>(prow, c2l);
+            const double rscale = kPrec == WLG_PRECISION_BF16 ? rec_rs[slot] : 1.0;
             double2 rb[kChunks];
 #pragma unroll
             for (int k = 0; k < kChunks; ++k) {
                 const int cc = lane + 32 * k;
-                rb[k] = cc < ld2 ? prow2[cc] : make_double2(0.0, 0.0);
+                rb[k] = cc < ld2 ? coupling_pair<kPrec>(prow, cc) : make_double2(0.0, 0.0);
             }
             // the previous attempt's add_flip_delta (m_prev = 0 leaves every field unchanged)
 #pragma unroll
@@ -805,7 +833,8 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
 
             // the next attempt's site, field and spin
             const int c = need_u ? c2 : c1;
-            const double m_eff = accepted ? m : 0.0;
+            // m_eff * scale is exact (m = +-2, the scale is an FP32 value)
+            const double m_eff = accepted ? (kPrec == WLG_PRECISION_BF16 ? m * rscale : m) : 0.0;
             const double h_next = fma(m_eff, need_u ? r2 : r1, need_u ? fc2 : fc1);
             const int s_next = (accepted && c == i) ? -si : (need_u ? s2 : s1);
             E = accepted ? Ep : E;
@@ -869,12 +898,12 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
             run(std::false_type{});
     }
     if (!failed) {  // the last attempt's field update
-        const double2* prow2 = reinterpret_cast<const double2*>(ring + static_cast<size_t>(prev_slot) * ld);
+        const JT* prow = ring + static_cast<size_t>(prev_slot) * row_stride;
 #pragma unroll
         for (int k = 0; k < kChunks; ++k) {
             const int cc = lane + 32 * k;
             if (cc < ld2) {
-                const double2 r = prow2[cc];
+                const double2 r = coupling_pair<kPrec>(prow, cc);
                 fr[k].x = fma(m_prev, r.x, fr[k].x);
                 fr[k].y = fma(m_prev, r.y, fr[k].y);
             }
@@ -966,52 +995,49 @@ SweepFn sweep_fn() {
 
 }  // namespace
 
-template <int K, bool kPow2>
+template <int K, bool kPow2, int kPrec>
 SweepFn split_fn() {
     static bool configured = false;
     if (!configured) {
-        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_dense_split_kernel<K, kPow2>),
+        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_dense_split_kernel<K, kPow2, kPrec>),
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
                    "cudaFuncSetAttribute");
         configured = true;
     }
-    return &sweep_dense_split_kernel<K, kPow2>;
+    return &sweep_dense_split_kernel<K, kPow2, kPrec>;
 }
 
-template <bool kPow2>
-SweepFn pick_split_width(int ld) {
-    switch ((ld + 63) / 64) {
-        case 1: return split_fn<1, kPow2>();
-        case 2: return split_fn<2, kPow2>();
-        case 3: return split_fn<3, kPow2>();
-        case 4: return split_fn<4, kPow2>();
-        case 5: return split_fn<5, kPow2>();
-        case 6: return split_fn<6, kPow2>();
-        case 7: return split_fn<7, kPow2>();
-        case 8: return split_fn<8, kPow2>();
-        case 9: return split_fn<9, kPow2>();
-        case 10: return split_fn<10, kPow2>();
-        case 11: return split_fn<11, kPow2>();
-        case 12: return split_fn<12, kPow2>();
-        case 13: return split_fn<13, kPow2>();
-        case 14: return split_fn<14, kPow2>();
-        case 15: return split_fn<15, kPow2>();
-        case 16: return split_fn<16, kPow2>();
-        default: return nullptr;
-    }
+// Chunks of 64 couplings per lane pass, rounded up to a power of two (unused chunks are
+// masked off), for ld <= 1024.
+template <bool kPow2, int kPrec>
+SweepFn pick_split_chunks(int ld) {
+    const int chunks = (ld + 63) / 64;
+    if (chunks <= 1) return split_fn<1, kPow2, kPrec>();
+    if (chunks <= 2) return split_fn<2, kPow2, kPrec>();
+    if (chunks <= 4) return split_fn<4, kPow2, kPrec>();
+    if (chunks <= 8) return split_fn<8, kPow2, kPrec>();
+    if (chunks <= 16) return split_fn<16, kPow2, kPrec>();
+    return nullptr;
 }
 
-// The split sweep for FP64 couplings with ld <= 1024 (chunks of 64 doubles per lane pass).
-SweepFn pick_split(int ld, bool pow2_width) {
-    return pow2_width ? pick_split_width<true>(ld) : pick_split_width<false>(ld);
+template <int kPrec>
+SweepFn pick_split_precision(int ld, bool pow2_width) {
+    return pow2_width ? pick_split_chunks<true, kPrec>(ld) : pick_split_chunks<false, kPrec>(ld);
+}
+
+// The split sweep for dense couplings with ld <= 1024.
+SweepFn pick_split(int ld, bool pow2_width, int precision) {
+    if (precision == WLG_PRECISION_FP32) return pick_split_precision<WLG_PRECISION_FP32>(ld, pow2_width);
+    if (precision == WLG_PRECISION_BF16) return pick_split_precision<WLG_PRECISION_BF16>(ld, pow2_width);
+    return pick_split_precision<WLG_PRECISION_FP64>(ld, pow2_width);
 }
 
 bool launch_sweep_dense(const EngineView& v, const WalkArgs& a, cudaStream_t stream) {
     const bool features = v.p.collect || v.p.nalivaiko;
     const size_t jbytes = v.precision == WLG_PRECISION_FP64 ? 8 : v.precision == WLG_PRECISION_FP32 ? 4 : 2;
-    if (!features && v.precision == WLG_PRECISION_FP64 && v.ld <= 1024) {  // the split sweep
-        SweepFn fn = pick_split(v.ld, v.grid.pow2_width != 0);
-        const size_t split_bytes = split_layout(v.ld, v.max_window_bins).total;
+    if (!features && v.ld <= 1024) {  // the split sweep
+        SweepFn fn = pick_split(v.ld, v.grid.pow2_width != 0, v.precision);
+        const size_t split_bytes = split_layout(v.ld, v.max_window_bins, jbytes).total;
         if (fn && split_bytes <= 227 * 1024) {
             fn<<<static_cast<unsigned>(a.count), 64, split_bytes, stream>>>(v, a);
             check_cuda(cudaGetLastError(), "sweep_dense_split_kernel");

@@ -104,3 +104,29 @@ def test_fp64_runs_have_no_recompute():
         e.run_epochs(3)
         rep = e.precision_report()
     assert rep["recompute_interval_attempts"] == 0 and rep["recomputes"] == 0
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "bf16"])
+def test_split_sweep_matches_ring_sweep(precision):
+    """Pilot statistics change no trajectory but route the dense sweep to the ring kernel
+    (sweep_dense_kernel) instead of the split kernel: the two must agree bit for bit."""
+    from helpers import snapshots_equal
+    s = System(simple_cubic_random(4, 4, 4, seed=3, periodic=True), 1.0, 0.0)
+
+    def run(collect: bool):
+        c = RunConfig(emin=-60, emax=60, bin_width=0.5, windows=2, walkers=2, overlap=0.5, seed=11)
+        c.wl = WlParameters(0.8, 100, 1e-6, 1000, 0, True)
+        c.wl.collect_window_statistics = collect
+        c.coupling_precision = precision
+        c.exchange_interval_mcs = 1.0
+        c.recompute_interval_mcs = 5.0
+        c.resolve_mcs(s.size())
+        with Engine(s, c) as e:
+            e.run_epochs(25)
+            return [e.snapshot(w) for w in range(4)], e.precision_report()
+
+    split, rep_a = run(False)
+    ring, rep_b = run(True)
+    for a, b in zip(split, ring):
+        assert snapshots_equal(a, b) == []
+    assert rep_a["max_field_drift"] == rep_b["max_field_drift"]
