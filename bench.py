@@ -336,13 +336,14 @@ def time_to_accuracy(tolerance: float = 0.05) -> dict:
     curves of random dipole clusters (8-12 spins, density 0.3-0.8, random axes); each of 6
     held-out clusters is then run from the flat start and from the learned start (ln f =
     1e-2) until max |d log g| against exact enumeration is <= tolerance."""
-    from replica_exchange_wang_landau_b200.warmstart import WarmStartModel, plain_dos, run_to_accuracy
+    from replica_exchange_wang_landau_b200.warmstart import WarmStartModel, plain_dos_many, run_to_accuracy
     t0 = time.perf_counter()
-    train = []
+    specs = []
     for k in range(1, 49):
         s = _cluster(k)
         emin, emax, w, _ = _enumerate(s)
-        train.append(plain_dos(s, emin, emax, w, seed=k, final_factor=1e-4))
+        specs.append((s, emin, emax, w, k))
+    train = plain_dos_many(specs, final_factor=1e-4)  # the 48 plain runs side by side in one batch
     model = WarmStartModel(hidden=(32, 32), seed=3)
     loss = model.fit(train, steps=4000, learning_rate=3e-3)
     train_s = time.perf_counter() - t0

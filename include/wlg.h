@@ -331,6 +331,20 @@ wlg_status wlg_walker_exchange_log_probability(wlg_engine* engine, uint64_t left
                                                uint64_t right, double* log_probability);
 wlg_status wlg_walker_swap(wlg_engine* engine, uint64_t left, uint64_t right);
 
+/* ---- batches of engines (no counterpart in the reference, which runs one instance) -----
+ * Engines created on the same device (different systems, sizes, windows or precisions)
+ * advanced together: one CUDA graph whose child graphs are the engines' captured epoch
+ * graphs, so a single launch runs every engine's next epochs side by side on the GPU.  An
+ * engine that has terminated keeps running no-op epochs.  Creating a batch runs one epoch
+ * of every engine whose epoch graph did not exist yet.  The engines must outlive the batch
+ * and must not be used elsewhere while wlg_batch_run_epochs runs. */
+typedef struct wlg_batch wlg_batch;
+wlg_status wlg_batch_create(wlg_engine* const* engines, uint64_t count, wlg_batch** out);
+/* Launches until every engine has terminated or about max_epochs epochs have run (each launch
+ * advances every engine by its epochs per graph); *launches = graph launches made. */
+wlg_status wlg_batch_run_epochs(wlg_batch* batch, uint64_t max_epochs, uint64_t* launches, int32_t* all_done);
+void wlg_batch_destroy(wlg_batch* batch);
+
 /* ---- the warm-start network (no counterpart in the reference) --------------------------
  * A small multilayer perceptron trained on DOS curves that plain runs produce: inputs are
  * per-bin features of a system (replica_exchange_wang_landau_b200/warmstart.py), the output

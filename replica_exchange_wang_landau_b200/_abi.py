@@ -211,6 +211,9 @@ SIGNATURES = {
     "wlg_engine_time_run": (_i32, [_vp, _u64, P(wlg_epoch_timing)]),
     "wlg_engine_precision_report": (_i32, [_vp, P(wlg_precision_report)]),
     "wlg_engine_warm_start": (_i32, [_vp, P(_dbl), _dbl]),
+    "wlg_batch_create": (_i32, [P(_vp), _u64, P(_vp)]),
+    "wlg_batch_run_epochs": (_i32, [_vp, _u64, P(_u64), P(_i32)]),
+    "wlg_batch_destroy": (None, [_vp]),
     "wlg_mlp_create": (_i32, [_i32, P(_i32), _u64, P(_vp)]),
     "wlg_mlp_destroy": (None, [_vp]),
     "wlg_mlp_parameter_count": (_u64, [_vp]),

@@ -512,4 +512,37 @@ wlg_status wlg_mlp_train(wlg_mlp* mlp, const float* x, const float* t, uint64_t 
     });
 }
 
+// ---- batches of engines (no counterpart in the reference) ---------------------------------
+
+struct wlg_batch {
+    wlg::Batch* impl;
+};
+
+wlg_status wlg_batch_create(wlg_engine* const* engines, uint64_t count, wlg_batch** out) {
+    return guarded([&] {
+        if (!engines || !out || count == 0) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        *out = nullptr;
+        std::vector<wlg::Engine*> list;
+        for (uint64_t k = 0; k < count; ++k) {
+            if (!engines[k]) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null engine in a batch");
+            list.push_back(engines[k]->impl);
+        }
+        wlg::check_cuda(cudaSetDevice(list[0]->device), "cudaSetDevice");
+        *out = new wlg_batch{new wlg::Batch(list)};
+    });
+}
+
+wlg_status wlg_batch_run_epochs(wlg_batch* batch, uint64_t max_epochs, uint64_t* launches, int32_t* all_done) {
+    return guarded([&] {
+        if (!batch) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null batch");
+        batch->impl->run_epochs(max_epochs, launches, all_done);
+    });
+}
+
+void wlg_batch_destroy(wlg_batch* batch) {
+    if (!batch) return;
+    delete batch->impl;
+    delete batch;
+}
+
 }  // extern "C"

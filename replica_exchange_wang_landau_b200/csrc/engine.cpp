@@ -502,19 +502,10 @@ void Engine::run_epochs(uint64_t max_epochs, uint64_t* epochs_run, int32_t* done
         }
         if (recompute_epochs_) chunk = std::min(chunk, std::max<uint64_t>(1, next_recompute_ - epochs_));
         launch_epochs(chunk);
-        check_device_error();
         budget -= std::min(budget, chunk);
-        if (recompute_epochs_ && !done_ && epochs_ >= next_recompute_) {
-            recompute_fields();
-            next_recompute_ = epochs_ + recompute_epochs_;
-        }
-        maybe_checkpoint();
-        print_progress(false);
+        after_epochs();
     }
-    if (done_) {
-        if (p_.collect) launch_flush_pending(view_, stream_);
-        print_progress(true);
-    }
+    if (done_) finish();
     if (epochs_run) *epochs_run = epochs_ - start;
     if (done) *done = done_ ? 1 : 0;
 }
@@ -543,6 +534,92 @@ void Engine::precision_report(wlg_precision_report* out) {
     out->bin_changes = r.bin_changes;
     std::memcpy(&out->max_field_drift, &r.max_field_drift_bits, sizeof(double));
     std::memcpy(&out->max_energy_drift, &r.max_energy_drift_bits, sizeof(double));
+}
+
+// Host work between launches: device errors, the mixed-precision recompute, the checkpoint
+// and the progress line.
+void Engine::after_epochs() {
+    check_device_error();
+    if (recompute_epochs_ && !done_ && epochs_ >= next_recompute_) {
+        recompute_fields();
+        next_recompute_ = epochs_ + recompute_epochs_;
+    }
+    maybe_checkpoint();
+    print_progress(false);
+}
+
+// Once, when the run has terminated: the representatives still pending and the final line.
+void Engine::finish() {
+    if (finished_) return;
+    finished_ = true;
+    if (p_.collect) launch_flush_pending(view_, stream_);
+    print_progress(true);
+}
+
+cudaGraph_t Engine::epoch_graph() {
+    if (!graph_exec_) {
+        WalkArgs a{};
+        a.first = 0;
+        a.count = static_cast<int32_t>(walkers_);
+        a.epoch_mode = 1;
+        a.smem_per_walker = static_cast<int32_t>(walker_smem_bytes(view_, smem_fields_, features_));
+        launch_walk(view_, a, walkers_per_block, stream_);  // sets the kernel attributes
+        launch_exchange(view_, stream_);
+        after_epochs();
+        build_graph();
+    }
+    return graph_;
+}
+
+void Engine::after_external_epochs() {
+    after_epochs();
+    if (done_) finish();
+}
+
+Batch::Batch(const std::vector<Engine*>& engines) : engines_(engines) {
+    if (engines_.empty()) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "an empty batch");
+    int device = 0;
+    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    for (size_t i = 0; i < engines_.size(); ++i) {
+        if (!engines_[i]) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "null engine in a batch");
+        if (engines_[i]->device != device)
+            throw WlgError(WLG_ERR_INVALID_ARGUMENT, "every engine of a batch must live on the current device");
+        for (size_t j = 0; j < i; ++j)
+            if (engines_[j] == engines_[i]) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "an engine appears twice");
+    }
+    check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    check_cuda(cudaGraphCreate(&graph_, 0), "cudaGraphCreate");
+    for (Engine* e : engines_) {
+        cudaGraphNode_t node = nullptr;
+        check_cuda(cudaGraphAddChildGraphNode(&node, graph_, nullptr, 0, e->epoch_graph()), "child graph");
+        epochs_per_launch_ = std::max<uint64_t>(epochs_per_launch_, static_cast<uint64_t>(e->epochs_per_graph));
+    }
+    check_cuda(cudaGraphInstantiate(&exec_, graph_, 0), "graph instantiate");
+}
+
+Batch::~Batch() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (exec_) cudaGraphExecDestroy(exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Batch::run_epochs(uint64_t max_epochs, uint64_t* launches, int32_t* all_done) {
+    uint64_t budget = max_epochs, n = 0;
+    auto everyone_done = [&] {
+        for (Engine* e : engines_)
+            if (!e->is_done()) return false;
+        return true;
+    };
+    while (budget > 0 && !everyone_done()) {
+        check_cuda(cudaGraphLaunch(exec_, stream_), "graph launch");
+        check_cuda(cudaStreamSynchronize(stream_), "batch");
+        ++n;
+        for (Engine* e : engines_) e->after_external_epochs();
+        budget -= std::min(budget, epochs_per_launch_);
+    }
+    if (launches) *launches = n;
+    if (all_done) *all_done = everyone_done() ? 1 : 0;
 }
 
 void Engine::run(wlg_run_totals* out) {

@@ -181,6 +181,26 @@ void mlp_forward(Mlp* m, const float* x, uint64_t batch, float* y);
 double mlp_gradients(Mlp* m, const float* x, const float* t, uint64_t batch, float* g);
 double mlp_train(Mlp* m, const float* x, const float* t, uint64_t batch, uint64_t steps, double lr);
 
+class Engine;
+
+// Several engines on one device advanced together: one CUDA graph whose child graphs are the
+// engines' captured epoch graphs, so one launch runs every instance's epochs side by side.
+class Batch {
+  public:
+    explicit Batch(const std::vector<Engine*>& engines);
+    ~Batch();
+    Batch(const Batch&) = delete;
+    Batch& operator=(const Batch&) = delete;
+    void run_epochs(uint64_t max_epochs, uint64_t* launches, int32_t* all_done);
+
+  private:
+    std::vector<Engine*> engines_;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t exec_ = nullptr;
+    cudaStream_t stream_ = nullptr;
+    uint64_t epochs_per_launch_ = 1;
+};
+
 // The engine: one REWL run on the current device.
 class Engine {
   public:
@@ -213,6 +233,12 @@ class Engine {
     void swap(uint64_t left, uint64_t right);
     void precision_report(wlg_precision_report* out);
     void warm_start(const double* log_g, double factor);
+    // batch support: the captured epoch graph (built on first use, after one direct epoch that
+    // primes the kernels) and the host work after epochs that a batch launch ran
+    cudaGraph_t epoch_graph();
+    void after_external_epochs();
+    bool is_done() const { return done_; }
+    uint64_t epoch_count() const { return epochs_; }
 
     // Launch shape (chosen by the autotuner or set explicitly).
     int walkers_per_block = 1;
@@ -226,6 +252,8 @@ class Engine {
     void build_graph();
     void maybe_checkpoint();
     void recompute_fields();
+    void after_epochs();
+    void finish();
     void print_progress(bool final_line);
     std::vector<WalkerState> download_states();
 
@@ -255,6 +283,7 @@ class Engine {
     bool checkpointing_ = false;
     uint64_t last_checkpoint_ = 0;
     bool done_ = false;
+    bool finished_ = false;
     uint64_t epochs_ = 0;
     double next_progress_ = 0.0;
     size_t progress_width_ = 0;

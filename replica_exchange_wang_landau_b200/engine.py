@@ -665,6 +665,47 @@ class Engine:
         _check(self._lib.wlg_walker_swap(self._h, left, right))
 
 
+class Batch:
+    """Engines on one device advanced together by single CUDA-graph launches (no counterpart
+    in the reference).  The engines must stay open while the batch is used."""
+
+    def __init__(self, engines: Sequence["Engine"]):
+        self.engines = list(engines)
+        self._lib = load_library()
+        arr = (C.c_void_p * len(self.engines))(*[e._h.value if isinstance(e._h, C.c_void_p) else e._h
+                                                 for e in self.engines])
+        h = C.c_void_p()
+        _check(self._lib.wlg_batch_create(arr, len(self.engines), C.byref(h)))
+        self._h = h
+
+    def run_epochs(self, max_epochs: int) -> bool:
+        """Runs until every engine has terminated or about max_epochs epochs; True if all did."""
+        launches, done = C.c_uint64(0), C.c_int32(0)
+        _check(self._lib.wlg_batch_run_epochs(self._h, int(max_epochs), C.byref(launches), C.byref(done)))
+        return bool(done.value)
+
+    def run(self) -> None:
+        while not self.run_epochs(1 << 62):
+            pass
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.wlg_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def run_rewl(system: System, config: RunConfig, walkers_per_block: int | None = None) -> RewlResult:
     """run_rewl (src/parallel.cpp:276-747) on one GPU."""
     with Engine(system, config, walkers_per_block) as e:

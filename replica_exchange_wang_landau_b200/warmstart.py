@@ -178,6 +178,32 @@ def plain_dos(system: System, emin: float, emax: float, width: float, seed: int 
     return DosSample(system, emin, emax, width, np.asarray(frag.log_g, np.float64), np.asarray(frag.valid, bool))
 
 
+def plain_dos_many(specs: Sequence[tuple], final_factor: float = 1e-4, walkers: int = 2) -> list:
+    """plain_dos for many (system, emin, emax, width, seed) at once: the engines run side by
+    side in one batch (one CUDA-graph launch advances all of them)."""
+    from .engine import Batch
+    engines = []
+    try:
+        for system, emin, emax, width, seed in specs:
+            c = RunConfig(emin=emin, emax=emax, bin_width=width, windows=1, walkers=walkers, seed=seed)
+            c.wl = WlParameters(0.8, 100, final_factor, 1000, 0, True)
+            c.exchange_interval_mcs = 10.0
+            c.max_mcs = 1e7
+            c.resolve_mcs(system.size())
+            engines.append(Engine(system, c))
+        with Batch(engines) as batch:
+            batch.run()
+        out = []
+        for (system, emin, emax, width, _), e in zip(specs, engines):
+            frag = e.fragment(0, allow_empty=True)
+            out.append(DosSample(system, emin, emax, width, np.asarray(frag.log_g, np.float64),
+                                 np.asarray(frag.valid, bool)))
+        return out
+    finally:
+        for e in engines:
+            e.close()
+
+
 @dataclass
 class WarmStartModel:
     """Feature and target scalings plus the trained network."""

@@ -11,7 +11,7 @@ import pytest
 from oracle import mlp_oracle
 from replica_exchange_wang_landau_b200.engine import Engine, Geometry, InvalidArgument, LogicError, RunConfig, System
 from replica_exchange_wang_landau_b200.geometry import random_sequential
-from replica_exchange_wang_landau_b200.warmstart import Mlp, WarmStartModel, plain_dos, run_to_accuracy
+from replica_exchange_wang_landau_b200.warmstart import Mlp, WarmStartModel, plain_dos_many, run_to_accuracy
 
 pytestmark = pytest.mark.gpu
 
@@ -82,10 +82,11 @@ def test_learned_warm_start_gain(oracle):
     (8-12 spins) starts 6 held-out clusters at ln f = 1e-2; over two seeds each, the learned
     runs reach max |d log g| <= 0.05 against exact enumeration in fewer total attempts than
     the same runs from the flat start (measured here: 0.66 of them)."""
-    train = []
+    specs = []
     for k in range(1, 49):
         s = _cluster(k)
-        train.append(plain_dos(s, *_grid(s), seed=k, final_factor=1e-4))
+        specs.append((s, *_grid(s), k))
+    train = plain_dos_many(specs, final_factor=1e-4)  # 48 engines in one batch
     model = WarmStartModel(hidden=(32, 32), seed=3)
     assert model.fit(train, steps=4000, learning_rate=3e-3) < 0.5
     flat = learned = 0
