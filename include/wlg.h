@@ -274,6 +274,20 @@ wlg_status wlg_engine_time_epochs(wlg_engine* engine, uint64_t epochs, wlg_epoch
  * and one after on the engine's stream: total_ms is the device time of the whole product
  * path; walk_ms and exchange_ms are 0.  No counterpart in the reference. */
 wlg_status wlg_engine_time_run(wlg_engine* engine, uint64_t epochs, wlg_epoch_timing* out);
+/* Result of the launch-shape autotuner. */
+typedef struct wlg_autotune_report {
+    int32_t walkers_per_block;   /* chosen walkers per CTA of the generic (CSR) sweep          */
+    int32_t epochs_per_graph;    /* chosen epochs per CUDA-graph replay                        */
+    double ms_per_epoch;         /* device time per epoch of the chosen shape                  */
+    uint64_t trials;             /* candidate shapes timed                                     */
+} wlg_autotune_report;
+
+/* Launch-shape autotuner: times candidate shapes (walkers per CTA 1-8 for the generic sweep,
+ * epochs per graph 4-64) on trial_epochs real epochs each through the product path and keeps
+ * the fastest.  The shape never changes results, so the trial epochs count as epochs of the
+ * run.  The exchange interval, which changes trajectories, is not tuned.  No counterpart in
+ * the reference. */
+wlg_status wlg_engine_autotune(wlg_engine* engine, uint64_t trial_epochs, wlg_autotune_report* out);
 /* Launch shape: walkers per CTA of the sweep kernel (1-8) and epochs per CUDA-graph
  * replay (>= 1); 0 leaves a value unchanged.  No counterpart in the reference. */
 wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block,

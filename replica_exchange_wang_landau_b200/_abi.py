@@ -151,6 +151,15 @@ class wlg_precision_report(C.Structure):
     ]
 
 
+class wlg_autotune_report(C.Structure):
+    _fields_ = [
+        ("walkers_per_block", C.c_int32),
+        ("epochs_per_graph", C.c_int32),
+        ("ms_per_epoch", C.c_double),
+        ("trials", C.c_uint64),
+    ]
+
+
 class wlg_snapshot(C.Structure):
     _fields_ = [
         ("walker_id", C.c_uint64),
@@ -180,6 +189,7 @@ STRUCTS = {
     "wlg_snapshot": wlg_snapshot,
     "wlg_epoch_timing": wlg_epoch_timing,
     "wlg_precision_report": wlg_precision_report,
+    "wlg_autotune_report": wlg_autotune_report,
 }
 
 P = C.POINTER
@@ -209,6 +219,7 @@ SIGNATURES = {
     "wlg_engine_totals": (_i32, [_vp, P(wlg_run_totals)]),
     "wlg_engine_time_epochs": (_i32, [_vp, _u64, P(wlg_epoch_timing)]),
     "wlg_engine_time_run": (_i32, [_vp, _u64, P(wlg_epoch_timing)]),
+    "wlg_engine_autotune": (_i32, [_vp, _u64, P(wlg_autotune_report)]),
     "wlg_engine_precision_report": (_i32, [_vp, P(wlg_precision_report)]),
     "wlg_engine_warm_start": (_i32, [_vp, P(_dbl), _dbl]),
     "wlg_batch_create": (_i32, [P(_vp), _u64, P(_vp)]),

@@ -346,6 +346,11 @@ wlg_status wlg_engine_time_run(wlg_engine* engine, uint64_t epochs, wlg_epoch_ti
     });
 }
 
+wlg_status wlg_engine_autotune(wlg_engine* engine, uint64_t trial_epochs, wlg_autotune_report* out) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] { engine->impl->autotune(trial_epochs, out); });
+}
+
 wlg_status wlg_engine_precision_report(wlg_engine* engine, wlg_precision_report* out) {
     WLG_ENGINE_GUARD(engine)
     return guarded([&] {

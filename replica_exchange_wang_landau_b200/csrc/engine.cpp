@@ -721,6 +721,48 @@ void Engine::set_launch(int wpb, int epg) {
     }
 }
 
+// Launch-shape autotuner: each candidate (walkers per CTA of the generic sweep, epochs per
+// graph replay) runs `trial_epochs` real epochs of this engine through the product path after
+// a warm-up replay that builds its graph, timed with device events; the fastest per epoch is
+// kept.  The launch shape never changes results, so the trial epochs are ordinary epochs of
+// the run.  (The exchange interval, which does change the sampled trajectories, is left as
+// configured.)
+void Engine::autotune(uint64_t trial_epochs, wlg_autotune_report* out) {
+    if (trial_epochs == 0) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "autotune needs at least one trial epoch");
+    const bool generic = sys_.csr || sys_.ld > 1024 || features_;
+    const int wpbs_generic[] = {1, 2, 4, 8};
+    const int wpbs_dense[] = {1};
+    const int* wpbs = generic ? wpbs_generic : wpbs_dense;
+    const int n_wpb = generic ? 4 : 1;
+    const int epgs[] = {4, 8, 16, 32, 64};
+    wlg_autotune_report r{};
+    double best = std::numeric_limits<double>::infinity();
+    int best_wpb = walkers_per_block, best_epg = epochs_per_graph;
+    for (int a = 0; a < n_wpb && !done_; ++a) {
+        for (int epg : epgs) {
+            if (done_) break;
+            set_launch(wpbs[a], epg);
+            wlg_epoch_timing t{};
+            time_run(static_cast<uint64_t>(epg), &t);  // builds and warms the graph
+            const uint64_t rounds = std::max<uint64_t>(1, (trial_epochs + epg - 1) / epg);
+            time_run(rounds * epg, &t);
+            ++r.trials;
+            if (t.epochs == 0) continue;
+            const double per_epoch = t.total_ms / static_cast<double>(t.epochs);
+            if (per_epoch < best) {
+                best = per_epoch;
+                best_wpb = wpbs[a];
+                best_epg = epg;
+            }
+        }
+    }
+    set_launch(best_wpb, best_epg);
+    r.walkers_per_block = best_wpb;
+    r.epochs_per_graph = best_epg;
+    r.ms_per_epoch = std::isfinite(best) ? best : 0.0;
+    if (out) *out = r;
+}
+
 void Engine::totals(wlg_run_totals* out) {
     Control ctl{};
     check_cuda(cudaMemcpyAsync(&ctl, d_ctl_.ptr, sizeof ctl, cudaMemcpyDeviceToHost, stream_), "copy control");

@@ -214,6 +214,7 @@ class Engine {
     void totals(wlg_run_totals* out);
     void time_epochs(uint64_t epochs, wlg_epoch_timing* out);
     void time_run(uint64_t epochs, wlg_epoch_timing* out);
+    void autotune(uint64_t trial_epochs, wlg_autotune_report* out);
     void set_launch(int walkers_per_block, int epochs_per_graph);
     uint64_t walkers() const { return walkers_; }
     uint64_t bins() const { return bins_; }

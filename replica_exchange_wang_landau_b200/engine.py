@@ -550,6 +550,13 @@ class Engine:
         _check(self._lib.wlg_engine_time_run(self._h, int(epochs), C.byref(t)))
         return {name: getattr(t, name) for name, _ in _abi.wlg_epoch_timing._fields_}
 
+    def autotune(self, trial_epochs: int = 16) -> dict:
+        """Times candidate launch shapes on real epochs and keeps the fastest (results are
+        unchanged by the launch shape)."""
+        r = _abi.wlg_autotune_report()
+        _check(self._lib.wlg_engine_autotune(self._h, int(trial_epochs), C.byref(r)))
+        return {name: getattr(r, name) for name, _ in _abi.wlg_autotune_report._fields_}
+
     def precision_report(self) -> dict:
         """Drift of a mixed-precision run over its periodic FP64 recomputes (zeros for FP64)."""
         r = _abi.wlg_precision_report()

@@ -48,6 +48,8 @@ int main(void) {
     F(wlg_precision_report, recompute_interval_attempts); F(wlg_precision_report, recomputes);
     F(wlg_precision_report, resynced); F(wlg_precision_report, deferred); F(wlg_precision_report, bin_changes);
     F(wlg_precision_report, max_field_drift); F(wlg_precision_report, max_energy_drift);
+    S(wlg_autotune_report); F(wlg_autotune_report, walkers_per_block); F(wlg_autotune_report, epochs_per_graph);
+    F(wlg_autotune_report, ms_per_epoch); F(wlg_autotune_report, trials);
     S(wlg_snapshot); F(wlg_snapshot, walker_id); F(wlg_snapshot, spins); F(wlg_snapshot, fields);
     F(wlg_snapshot, energy); F(wlg_snapshot, log_g); F(wlg_snapshot, histogram); F(wlg_snapshot, active);
     F(wlg_snapshot, factor); F(wlg_snapshot, attempted); F(wlg_snapshot, accepted); F(wlg_snapshot, forced_accepted);

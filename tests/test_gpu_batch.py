@@ -57,3 +57,24 @@ def test_batch_rejects_duplicates():
     with Engine(s, c) as e:
         with pytest.raises(Exception):
             Batch([e, e])
+
+
+@pytest.mark.parametrize("cutoff", [0.0, 1.8])
+def test_autotune_keeps_results(cutoff):
+    """The launch-shape autotuner changes speed only: the run's results are bit-identical."""
+    s = System(simple_cubic_random(4, 4, 4, seed=3, periodic=True), 1.0, cutoff)
+    c = RunConfig(emin=-60, emax=60, bin_width=0.5, windows=2, walkers=2, overlap=0.5, seed=9)
+    c.wl = WlParameters(0.8, 100, 1e-3, 1000, 0, True)
+    c.exchange_interval_mcs = 2.0
+    c.max_mcs = 4000.0
+    c.resolve_mcs(s.size())
+    with Engine(s, c) as e:
+        e.run()
+        plain = [e.snapshot(w) for w in range(4)]
+    with Engine(s, c) as e:
+        r = e.autotune(4)
+        assert r["epochs_per_graph"] in (4, 8, 16, 32, 64) and 1 <= r["walkers_per_block"] <= 8
+        assert r["trials"] >= 5 and r["ms_per_epoch"] > 0
+        e.run()
+        for w in range(4):
+            assert snapshots_equal(e.snapshot(w), plain[w]) == []
