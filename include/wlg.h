@@ -345,6 +345,41 @@ wlg_status wlg_walker_exchange_log_probability(wlg_engine* engine, uint64_t left
                                                uint64_t right, double* log_probability);
 wlg_status wlg_walker_swap(wlg_engine* engine, uint64_t left, uint64_t right);
 
+/* ---- stitching and output (wl::stitch_dos, src/analysis.cpp:45-130; write_dos_csv and
+ * write_fragment_csv, src/io.cpp:398-421) ----------------------------------------------- */
+/* One window's fragment: whole-grid arrays (grid-bins entries each), window [begin, end). */
+typedef struct wlg_fragment_view {
+    uint64_t window_begin, window_end;
+    const double* log_g;
+    const uint64_t* histogram;
+    const double* standard_error;
+    const uint8_t* valid;
+} wlg_fragment_view;
+/* Quality of one join (an addition: the reference reports only the join bins): over the
+ * overlap of the two fragments, the number of common valid bins, the RMSE and the maximum
+ * absolute difference of the aligned curves, and the slope mismatch at the join (NaN when
+ * the slope criterion found no bin and the overlap midpoint was used). */
+typedef struct wlg_join_quality {
+    uint64_t join_bin;
+    uint64_t common_bins;
+    double rmse;
+    double max_abs_difference;
+    double slope_difference;
+} wlg_join_quality;
+/* Stitches `count` fragments (any order) into whole-grid outputs; joins gets count-1 entries
+ * (may be NULL).  complete_range normalises sum g = 2^spin_count, else the peak is 0. */
+wlg_status wlg_stitch_dos(double emin, double emax, double width, const wlg_fragment_view* fragments,
+                          uint64_t count, int32_t complete_range, uint64_t spin_count, double* log_g,
+                          uint64_t* histogram, double* standard_error, uint8_t* valid, wlg_join_quality* joins,
+                          int32_t* fully_normalized);
+/* The reference's <prefix>_dos.csv, byte for byte. */
+wlg_status wlg_write_dos_csv(const char* path, double emin, double width, uint64_t bins, const double* log_g,
+                             const uint64_t* histogram, const double* standard_error, const uint8_t* valid);
+/* The reference's <prefix>_window_<w>.csv of one fragment (bins [begin, end)). */
+wlg_status wlg_write_fragment_csv(const char* path, double emin, double width, uint64_t window_id,
+                                  uint64_t window_begin, uint64_t window_end, const double* log_g,
+                                  const uint64_t* histogram, const double* standard_error, const uint8_t* valid);
+
 /* ---- batches of engines (no counterpart in the reference, which runs one instance) -----
  * Engines created on the same device (different systems, sizes, windows or precisions)
  * advanced together: one CUDA graph whose child graphs are the engines' captured epoch

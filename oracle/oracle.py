@@ -264,6 +264,10 @@ class Reference(_Checker):
             "ref_result_sampling": (C.c_int, [_vp, _u64, P(_dbl), P(_u64), P(_u64), P(_u64)]),
             "ref_result_representatives": (_u64, [_vp, P(_dbl), P(C.c_int8), _u64]),
             "ref_adapt_windows": (C.c_int, [_vp, _dbl, _dbl, _dbl, _u64, _dbl, P(_u64), _cp, _sz]),
+            "ref_stitch_dos": (C.c_int, [_dbl, _dbl, _dbl, P(_abi.wlg_fragment_view), _u64, C.c_int, _u64, P(_dbl),
+                                         P(_u64), P(_dbl), P(C.c_uint8), P(_u64), C.c_char_p, _cp, _sz]),
+            "ref_write_fragment_csv": (C.c_int, [C.c_char_p, _dbl, _dbl, _dbl, P(_abi.wlg_fragment_view), _u64, _cp,
+                                                 _sz]),
         }
         for name, (res, args) in sig.items():
             getattr(L, name).restype = res
@@ -271,6 +275,24 @@ class Reference(_Checker):
 
     def set_threads(self, threads: int) -> int:
         return int(self.lib.ref_set_threads(int(threads)))
+
+    def stitch_dos(self, views, emin, emax, width, complete_range: bool, spins: int, dos_csv: str = ""):
+        """wl::stitch_dos on wlg_fragment_view inputs; also writes <dos_csv> when given."""
+        bins = int(round((emax - emin) / width))
+        lg, se = np.zeros(bins), np.zeros(bins)
+        h, v = np.zeros(bins, np.uint64), np.zeros(bins, np.uint8)
+        joins = np.zeros(max(1, len(views) - 1), np.uint64)
+        arr = (_abi.wlg_fragment_view * len(views))(*views)
+        err = _err()
+        _raise(self.lib.ref_stitch_dos(emin, emax, width, arr, len(views), int(complete_range), spins, _dptr(lg),
+                                       _u64ptr(h), _dptr(se), _u8ptr(v), _u64ptr(joins), str(dos_csv).encode(), err,
+                                       len(err)), err)
+        return lg, h, se, v, joins[:len(views) - 1]
+
+    def write_fragment_csv(self, path, view, emin, emax, width, window_id: int) -> None:
+        err = _err()
+        _raise(self.lib.ref_write_fragment_csv(str(path).encode(), emin, emax, width, C.byref(view), window_id, err,
+                                               len(err)), err)
 
     def couplings(self, system: System) -> np.ndarray:
         n = system.size()

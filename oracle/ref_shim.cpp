@@ -401,4 +401,46 @@ int ref_adapt_windows(void* handle, double emin, double emax, double width, uint
     } catch (const std::exception& e) { put_error(err, errlen, e.what()); return status_of(e); }
 }
 
+// wl::stitch_dos and the DOS / fragment writers (src/analysis.cpp:45-130, src/io.cpp:398-421),
+// for the byte-level comparison of the stitched output.
+static std::vector<wl::DosFragment> fragments_from(const wlg_fragment_view* f, uint64_t count, uint64_t bins) {
+    std::vector<wl::DosFragment> out(count);
+    for (uint64_t k = 0; k < count; ++k) {
+        out[k].window = {f[k].window_begin, f[k].window_end};
+        out[k].log_g.assign(f[k].log_g, f[k].log_g + bins);
+        out[k].histogram.assign(f[k].histogram, f[k].histogram + bins);
+        out[k].standard_error.assign(f[k].standard_error, f[k].standard_error + bins);
+        out[k].valid.assign(f[k].valid, f[k].valid + bins);
+    }
+    return out;
+}
+
+int ref_stitch_dos(double emin, double emax, double width, const wlg_fragment_view* f, uint64_t count, int complete,
+                   uint64_t spins, double* lg, uint64_t* h, double* se, uint8_t* v, uint64_t* joins,
+                   const char* dos_csv, char* err, size_t errlen) {
+    try {
+        const wl::EnergyGrid grid{emin, emax, width};
+        const auto bins = grid.bins();
+        const auto frags = fragments_from(f, count, bins);
+        const auto dos = wl::stitch_dos(grid, frags, complete != 0, spins);
+        std::copy(dos.log_g.begin(), dos.log_g.end(), lg);
+        std::copy(dos.histogram.begin(), dos.histogram.end(), h);
+        std::copy(dos.standard_error.begin(), dos.standard_error.end(), se);
+        std::copy(dos.valid.begin(), dos.valid.end(), v);
+        for (std::size_t k = 0; k < dos.join_bins.size(); ++k) joins[k] = dos.join_bins[k];
+        if (dos_csv && dos_csv[0]) wl::write_dos_csv(dos_csv, dos);
+        return 0;
+    } catch (const std::exception& e) { put_error(err, errlen, e.what()); return status_of(e); }
+}
+
+int ref_write_fragment_csv(const char* path, double emin, double emax, double width, const wlg_fragment_view* f,
+                           uint64_t window_id, char* err, size_t errlen) {
+    try {
+        const wl::EnergyGrid grid{emin, emax, width};
+        const auto frags = fragments_from(f, 1, grid.bins());
+        wl::write_fragment_csv(path, grid, frags[0], window_id);
+        return 0;
+    } catch (const std::exception& e) { put_error(err, errlen, e.what()); return status_of(e); }
+}
+
 } // extern "C"

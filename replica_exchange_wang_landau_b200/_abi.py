@@ -160,6 +160,27 @@ class wlg_autotune_report(C.Structure):
     ]
 
 
+class wlg_fragment_view(C.Structure):
+    _fields_ = [
+        ("window_begin", C.c_uint64),
+        ("window_end", C.c_uint64),
+        ("log_g", C.POINTER(C.c_double)),
+        ("histogram", C.POINTER(C.c_uint64)),
+        ("standard_error", C.POINTER(C.c_double)),
+        ("valid", C.POINTER(C.c_uint8)),
+    ]
+
+
+class wlg_join_quality(C.Structure):
+    _fields_ = [
+        ("join_bin", C.c_uint64),
+        ("common_bins", C.c_uint64),
+        ("rmse", C.c_double),
+        ("max_abs_difference", C.c_double),
+        ("slope_difference", C.c_double),
+    ]
+
+
 class wlg_snapshot(C.Structure):
     _fields_ = [
         ("walker_id", C.c_uint64),
@@ -190,6 +211,8 @@ STRUCTS = {
     "wlg_epoch_timing": wlg_epoch_timing,
     "wlg_precision_report": wlg_precision_report,
     "wlg_autotune_report": wlg_autotune_report,
+    "wlg_fragment_view": wlg_fragment_view,
+    "wlg_join_quality": wlg_join_quality,
 }
 
 P = C.POINTER
@@ -222,6 +245,11 @@ SIGNATURES = {
     "wlg_engine_autotune": (_i32, [_vp, _u64, P(wlg_autotune_report)]),
     "wlg_engine_precision_report": (_i32, [_vp, P(wlg_precision_report)]),
     "wlg_engine_warm_start": (_i32, [_vp, P(_dbl), _dbl]),
+    "wlg_stitch_dos": (_i32, [_dbl, _dbl, _dbl, P(wlg_fragment_view), _u64, _i32, _u64, P(_dbl), P(_u64), P(_dbl),
+                               P(C.c_uint8), P(wlg_join_quality), P(_i32)]),
+    "wlg_write_dos_csv": (_i32, [C.c_char_p, _dbl, _dbl, _u64, P(_dbl), P(_u64), P(_dbl), P(C.c_uint8)]),
+    "wlg_write_fragment_csv": (_i32, [C.c_char_p, _dbl, _dbl, _u64, _u64, _u64, P(_dbl), P(_u64), P(_dbl),
+                                      P(C.c_uint8)]),
     "wlg_batch_create": (_i32, [P(_vp), _u64, P(_vp)]),
     "wlg_batch_run_epochs": (_i32, [_vp, _u64, P(_u64), P(_i32)]),
     "wlg_batch_destroy": (None, [_vp]),

@@ -550,4 +550,38 @@ void wlg_batch_destroy(wlg_batch* batch) {
     delete batch;
 }
 
+// ---- stitching and output -------------------------------------------------------------
+
+wlg_status wlg_stitch_dos(double emin, double emax, double width, const wlg_fragment_view* fragments,
+                          uint64_t count, int32_t complete_range, uint64_t spin_count, double* log_g,
+                          uint64_t* histogram, double* standard_error, uint8_t* valid, wlg_join_quality* joins,
+                          int32_t* fully_normalized) {
+    return guarded([&] {
+        if (!log_g || !histogram || !standard_error || !valid)
+            throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null output");
+        wlg::stitch_dos(emin, emax, width, fragments, count, complete_range != 0, spin_count, log_g, histogram,
+                        standard_error, valid, joins, fully_normalized);
+    });
+}
+
+wlg_status wlg_write_dos_csv(const char* path, double emin, double width, uint64_t bins, const double* log_g,
+                             const uint64_t* histogram, const double* standard_error, const uint8_t* valid) {
+    return guarded([&] {
+        if (!path || !log_g || !histogram || !standard_error || !valid)
+            throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        wlg::write_dos_csv(path, emin, width, bins, log_g, histogram, standard_error, valid);
+    });
+}
+
+wlg_status wlg_write_fragment_csv(const char* path, double emin, double width, uint64_t window_id,
+                                  uint64_t window_begin, uint64_t window_end, const double* log_g,
+                                  const uint64_t* histogram, const double* standard_error, const uint8_t* valid) {
+    return guarded([&] {
+        if (!path || !log_g || !histogram || !standard_error || !valid)
+            throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        wlg::write_fragment_csv(path, emin, width, window_id, window_begin, window_end, log_g, histogram,
+                                standard_error, valid);
+    });
+}
+
 }  // extern "C"

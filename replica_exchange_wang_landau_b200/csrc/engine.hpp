@@ -97,6 +97,16 @@ bool load_checkpoint_file(const std::string& path, std::vector<int8_t>& spins, s
                           std::vector<double>& log_g, std::vector<uint64_t>& hist, std::vector<uint8_t>& active,
                           wlg_snapshot& scalars, std::string& error);
 
+// stitch.cpp
+void stitch_dos(double emin, double emax, double width, const wlg_fragment_view* fragments, uint64_t count,
+                bool complete_range, uint64_t spins, double* log_g, uint64_t* histogram, double* standard_error,
+                uint8_t* valid, wlg_join_quality* joins, int32_t* fully_normalized);
+void write_dos_csv(const char* path, double emin, double width, uint64_t bins, const double* log_g,
+                   const uint64_t* histogram, const double* standard_error, const uint8_t* valid);
+void write_fragment_csv(const char* path, double emin, double width, uint64_t window_id, uint64_t begin,
+                        uint64_t end, const double* log_g, const uint64_t* histogram, const double* standard_error,
+                        const uint8_t* valid);
+
 // physics.cu
 void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream);
 // noalloc.cu: local fields with every intermediate in a static device array.

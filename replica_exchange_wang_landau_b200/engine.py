@@ -760,3 +760,67 @@ def load_checkpoint(path: str) -> Snapshot:
     s, arrays = Snapshot._empty(int(n.value), int(b.value))
     _check(lib.wlg_checkpoint_load(str(path).encode(), C.byref(s), C.byref(n), C.byref(b)))
     return Snapshot._from(s, arrays)
+
+
+# ---- stitching and output (wl::stitch_dos, src/analysis.cpp:45-130; src/io.cpp:398-421) ---
+
+
+@dataclass
+class DensityOfStates:
+    """wl::DensityOfStates (include/wl/analysis.hpp:40-48) plus the per-join overlap quality."""
+
+    emin: float
+    emax: float
+    width: float
+    log_g: np.ndarray
+    histogram: np.ndarray
+    standard_error: np.ndarray
+    valid: np.ndarray
+    join_bins: list
+    joins: list
+    fully_normalized: bool
+
+
+def _fragment_view(frag: DosFragment):
+    arrays = (np.ascontiguousarray(frag.log_g, dtype=np.float64), np.ascontiguousarray(frag.histogram, dtype=np.uint64),
+              np.ascontiguousarray(frag.standard_error, dtype=np.float64),
+              np.ascontiguousarray(frag.valid, dtype=np.uint8))
+    v = _abi.wlg_fragment_view(int(frag.window[0]), int(frag.window[1]), _dptr(arrays[0]), _u64ptr(arrays[1]),
+                               _dptr(arrays[2]), _u8ptr(arrays[3]))
+    return v, arrays
+
+
+def stitch_dos(fragments: Sequence[DosFragment], emin: float, emax: float, width: float,
+               complete_range: bool = False, spin_count: int = 0) -> DensityOfStates:
+    """stitch_dos (src/analysis.cpp:45-130), bit-identical, with the overlap quality of each join."""
+    bins = grid_bins(emin, emax, width)
+    views, keep = [], []
+    for f in fragments:
+        v, arrays = _fragment_view(f)
+        views.append(v)
+        keep.append(arrays)
+    lg, se = np.empty(bins), np.empty(bins)
+    h, ok = np.empty(bins, np.uint64), np.empty(bins, np.uint8)
+    joins = (_abi.wlg_join_quality * max(1, len(views) - 1))()
+    full = C.c_int32(0)
+    arr = (_abi.wlg_fragment_view * max(1, len(views)))(*views)
+    _check(load_library().wlg_stitch_dos(emin, emax, width, arr, len(views), int(complete_range), int(spin_count),
+                                         _dptr(lg), _u64ptr(h), _dptr(se), _u8ptr(ok), joins, C.byref(full)))
+    q = [{name: getattr(joins[k], name) for name, _ in _abi.wlg_join_quality._fields_} for k in range(len(views) - 1)]
+    return DensityOfStates(emin, emax, width, lg, h, se, ok, [j["join_bin"] for j in q], q, bool(full.value))
+
+
+def write_dos_csv(path: str, dos: DensityOfStates) -> None:
+    """<prefix>_dos.csv in the reference's format (src/io.cpp:398-408), byte for byte."""
+    _check(load_library().wlg_write_dos_csv(str(path).encode(), dos.emin, dos.width, len(dos.log_g),
+                                            _dptr(np.ascontiguousarray(dos.log_g, np.float64)),
+                                            _u64ptr(np.ascontiguousarray(dos.histogram, np.uint64)),
+                                            _dptr(np.ascontiguousarray(dos.standard_error, np.float64)),
+                                            _u8ptr(np.ascontiguousarray(dos.valid, np.uint8))))
+
+
+def write_fragment_csv(path: str, fragment: DosFragment, emin: float, width: float, window_id: int) -> None:
+    """<prefix>_window_<w>.csv in the reference's format (src/io.cpp:410-421), byte for byte."""
+    v, arrays = _fragment_view(fragment)
+    _check(load_library().wlg_write_fragment_csv(str(path).encode(), emin, width, int(window_id), v.window_begin,
+                                                 v.window_end, v.log_g, v.histogram, v.standard_error, v.valid))

@@ -50,6 +50,11 @@ int main(void) {
     F(wlg_precision_report, max_field_drift); F(wlg_precision_report, max_energy_drift);
     S(wlg_autotune_report); F(wlg_autotune_report, walkers_per_block); F(wlg_autotune_report, epochs_per_graph);
     F(wlg_autotune_report, ms_per_epoch); F(wlg_autotune_report, trials);
+    S(wlg_fragment_view); F(wlg_fragment_view, window_begin); F(wlg_fragment_view, window_end);
+    F(wlg_fragment_view, log_g); F(wlg_fragment_view, histogram); F(wlg_fragment_view, standard_error);
+    F(wlg_fragment_view, valid);
+    S(wlg_join_quality); F(wlg_join_quality, join_bin); F(wlg_join_quality, common_bins); F(wlg_join_quality, rmse);
+    F(wlg_join_quality, max_abs_difference); F(wlg_join_quality, slope_difference);
     S(wlg_snapshot); F(wlg_snapshot, walker_id); F(wlg_snapshot, spins); F(wlg_snapshot, fields);
     F(wlg_snapshot, energy); F(wlg_snapshot, log_g); F(wlg_snapshot, histogram); F(wlg_snapshot, active);
     F(wlg_snapshot, factor); F(wlg_snapshot, attempted); F(wlg_snapshot, accepted); F(wlg_snapshot, forced_accepted);
