@@ -274,6 +274,17 @@ wlg_status wlg_engine_time_epochs(wlg_engine* engine, uint64_t epochs, wlg_epoch
  * and one after on the engine's stream: total_ms is the device time of the whole product
  * path; walk_ms and exchange_ms are 0.  No counterpart in the reference. */
 wlg_status wlg_engine_time_run(wlg_engine* engine, uint64_t epochs, wlg_epoch_timing* out);
+/* Multi-walker run checkpoint (an extension: the reference checkpoints single-walker runs
+ * only, src/parallel.cpp:354).  save writes every walker's full state (configuration,
+ * estimators, counters, RNG), the epoch and exchange counters and the mixed-precision
+ * recompute schedule, atomically (a temporary file renamed over `path`); load restores them
+ * into an engine created with the same system, grid, windows, walkers, precision and
+ * options, after which the run continues bit for bit as if it had not stopped.  With
+ * checkpoint_path set and more than one walker, the engine restores from that file at
+ * creation when it exists and writes it every checkpoint_interval_attempts. */
+wlg_status wlg_engine_save_run(wlg_engine* engine, const char* path);
+wlg_status wlg_engine_load_run(wlg_engine* engine, const char* path);
+
 /* Result of the launch-shape autotuner. */
 typedef struct wlg_autotune_report {
     int32_t walkers_per_block;   /* chosen walkers per CTA of the generic (CSR) sweep          */

@@ -243,6 +243,8 @@ SIGNATURES = {
     "wlg_engine_time_epochs": (_i32, [_vp, _u64, P(wlg_epoch_timing)]),
     "wlg_engine_time_run": (_i32, [_vp, _u64, P(wlg_epoch_timing)]),
     "wlg_engine_autotune": (_i32, [_vp, _u64, P(wlg_autotune_report)]),
+    "wlg_engine_save_run": (_i32, [_vp, C.c_char_p]),
+    "wlg_engine_load_run": (_i32, [_vp, C.c_char_p]),
     "wlg_engine_precision_report": (_i32, [_vp, P(wlg_precision_report)]),
     "wlg_engine_warm_start": (_i32, [_vp, P(_dbl), _dbl]),
     "wlg_stitch_dos": (_i32, [_dbl, _dbl, _dbl, P(wlg_fragment_view), _u64, _i32, _u64, P(_dbl), P(_u64), P(_dbl),

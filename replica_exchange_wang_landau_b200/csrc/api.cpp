@@ -346,6 +346,22 @@ wlg_status wlg_engine_time_run(wlg_engine* engine, uint64_t epochs, wlg_epoch_ti
     });
 }
 
+wlg_status wlg_engine_save_run(wlg_engine* engine, const char* path) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] {
+        if (!path || !path[0]) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "empty checkpoint path");
+        engine->impl->save_run(path);
+    });
+}
+
+wlg_status wlg_engine_load_run(wlg_engine* engine, const char* path) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] {
+        if (!path || !path[0]) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "empty checkpoint path");
+        engine->impl->load_run(path);
+    });
+}
+
 wlg_status wlg_engine_autotune(wlg_engine* engine, uint64_t trial_epochs, wlg_autotune_report* out) {
     WLG_ENGINE_GUARD(engine)
     return guarded([&] { engine->impl->autotune(trial_epochs, out); });

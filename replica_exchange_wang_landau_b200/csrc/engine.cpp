@@ -9,6 +9,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <fstream>
 #include <iostream>
 #include <limits>
 #include <mutex>
@@ -134,6 +135,21 @@ Engine::Engine(const wlg_system& system, const wlg_run_config& c) : cfg_(c) {
     cfg_.initial_spins_present = nullptr;
     cfg_.checkpoint_path = nullptr;
 
+    // fingerprint of the system, so that a run checkpoint is never restored onto another one
+    {
+        uint64_t h = 1469598103934665603ULL;
+        auto mix = [&h](const void* p, size_t bytes) {
+            const unsigned char* c = static_cast<const unsigned char*>(p);
+            for (size_t k = 0; k < bytes; ++k) h = (h ^ c[k]) * 1099511628211ULL;
+        };
+        mix(system.positions, system.n * 24);
+        mix(system.axes, system.n * 24);
+        mix(system.box, sizeof system.box);
+        mix(&system.periodic, sizeof system.periodic);
+        mix(&system.coupling_scale, sizeof system.coupling_scale);
+        mix(&system.cutoff, sizeof system.cutoff);
+        system_hash_ = h;
+    }
     require_device();
     check_cuda(cudaGetDevice(&device), "cudaGetDevice");
     check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
@@ -335,6 +351,20 @@ void Engine::initialise_walkers(const wlg_run_config& c) {
         ctor_failure(w, m.str());
     }
 
+    // multi-walker checkpoint (an extension: the reference checkpoints 1 x 1 runs only)
+    checkpointing_all_ = !checkpoint_path_.empty() && W > 1;
+    if (checkpointing_all_) {
+        std::ifstream probe(checkpoint_path_, std::ios::binary);
+        if (probe) {
+            probe.close();
+            try {
+                load_run(checkpoint_path_);
+            } catch (const std::exception& e) {
+                std::cerr << "warning: run checkpoint was not restored: " << e.what() << "; starting a new run\n";
+            }
+        }
+    }
+
     // single-walker checkpoint restore (src/parallel.cpp:354-360)
     checkpointing_ = !checkpoint_path_.empty() && windows_ == 1 && wpw_ == 1;
     if (checkpointing_) {
@@ -436,6 +466,16 @@ void Engine::launch_epochs(uint64_t count) {
 }
 
 void Engine::maybe_checkpoint() {
+    if (checkpointing_all_) {
+        WalkerState st{};
+        check_cuda(cudaMemcpyAsync(&st, d_ws_.ptr, sizeof st, cudaMemcpyDeviceToHost, stream_), "copy state");
+        check_cuda(cudaStreamSynchronize(stream_), "sync");
+        if (st.attempted - last_checkpoint_ >= cfg_.checkpoint_interval_attempts) {
+            save_run(checkpoint_path_);
+            last_checkpoint_ = st.attempted;
+        }
+        return;
+    }
     if (!checkpointing_) return;
     WalkerState st{};
     check_cuda(cudaMemcpyAsync(&st, d_ws_.ptr, sizeof st, cudaMemcpyDeviceToHost, stream_), "copy state");
@@ -1106,6 +1146,202 @@ void Engine::warm_start(const double* log_g, double factor) {
                                stream_),
                "copy states");
     check_cuda(cudaStreamSynchronize(stream_), "sync");
+}
+
+// ---- multi-walker run checkpoint -------------------------------------------------------
+//
+// Binary layout (host byte order): RunHeader, window bounds (2 x windows uint64), Control,
+// PrecisionReport, then per walker in walker order WalkerState and the walker's spins (ld
+// bytes) and fields (ld doubles), then the whole-grid estimator arrays (W x bins: log g,
+// H, active; with pilot statistics or the Nalivaiko mask also the refinement mask, the
+// squared displacements and their sample counts; with pilot statistics the representative
+// bank).  A restore puts walker w's configuration in slot w.
+
+namespace {
+struct RunHeader {
+    char magic[8];
+    uint64_t walkers, windows, n, ld, bins, seed, system_hash;
+    int32_t precision, features, collect, pad;
+    double emin, emax, width;
+    uint64_t recomputes, next_recompute_in;  // epochs until the next FP64 recompute
+};
+constexpr char kRunMagic[8] = {'W', 'L', 'G', 'R', 'U', 'N', '0', '1'};
+
+template <class T> void put_raw(std::ofstream& out, const T* p, size_t count) {
+    out.write(reinterpret_cast<const char*>(p), static_cast<std::streamsize>(count * sizeof(T)));
+}
+template <class T> void get_raw(std::ifstream& in, T* p, size_t count) {
+    in.read(reinterpret_cast<char*>(p), static_cast<std::streamsize>(count * sizeof(T)));
+    if (!in) throw WlgError(WLG_ERR_IO, "Run checkpoint is truncated");
+}
+template <class T> std::vector<T> download(const DeviceBuffer& b, size_t count, cudaStream_t s) {
+    std::vector<T> v(count);
+    if (count) check_cuda(cudaMemcpyAsync(v.data(), b.ptr, count * sizeof(T), cudaMemcpyDeviceToHost, s), "copy");
+    return v;
+}
+template <class T> void upload(DeviceBuffer& b, const std::vector<T>& v, cudaStream_t s) {
+    if (!v.empty())
+        check_cuda(cudaMemcpyAsync(b.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "copy");
+}
+}  // namespace
+
+void Engine::save_run(const std::string& path) {
+    const size_t W = walkers_, B = bins_, ld = sys_.ld, WB = W * B;
+    const size_t R = p_.collect ? W * kRepresentatives : 0;
+    Control ctl{};
+    PrecisionReport rep{};
+    check_cuda(cudaMemcpyAsync(&ctl, d_ctl_.ptr, sizeof ctl, cudaMemcpyDeviceToHost, stream_), "copy control");
+    check_cuda(cudaMemcpyAsync(&rep, d_prec_.ptr, sizeof rep, cudaMemcpyDeviceToHost, stream_), "copy report");
+    std::vector<WalkerState> st = download<WalkerState>(d_ws_, W, stream_);
+    std::vector<int8_t> spins = download<int8_t>(d_spins_, W * ld, stream_);
+    std::vector<double> fields = download<double>(d_fields_, W * ld, stream_);
+    std::vector<double> lg = download<double>(d_log_g_, WB, stream_);
+    std::vector<uint64_t> h = download<uint64_t>(d_hist_, WB, stream_);
+    std::vector<uint8_t> act = download<uint8_t>(d_active_, WB, stream_);
+    std::vector<uint8_t> ref = download<uint8_t>(d_refine_, features_ ? WB : 0, stream_);
+    std::vector<double> sq = download<double>(d_sqdisp_, features_ ? WB : 0, stream_);
+    std::vector<uint64_t> ds = download<uint64_t>(d_dsamples_, features_ ? WB : 0, stream_);
+    std::vector<double> re = download<double>(d_rep_energy_, R, stream_), rd = download<double>(d_rep_dist_, R, stream_),
+                        rt = download<double>(d_rep_target_, R, stream_);
+    std::vector<uint8_t> rp = download<uint8_t>(d_rep_present_, R, stream_);
+    std::vector<int8_t> rs = download<int8_t>(d_rep_spins_, R * ld, stream_);
+    check_cuda(cudaStreamSynchronize(stream_), "checkpoint");
+
+    RunHeader hd{};
+    std::memcpy(hd.magic, kRunMagic, 8);
+    hd.walkers = W;
+    hd.windows = windows_;
+    hd.n = sys_.n;
+    hd.ld = ld;
+    hd.bins = B;
+    hd.seed = p_.seed;
+    hd.system_hash = system_hash_;
+    hd.precision = precision_;
+    hd.features = features_ ? 1 : 0;
+    hd.collect = p_.collect ? 1 : 0;
+    hd.emin = cfg_.emin;
+    hd.emax = cfg_.emax;
+    hd.width = cfg_.bin_width;
+    hd.recomputes = recomputes_;
+    hd.next_recompute_in = next_recompute_ > epochs_ ? next_recompute_ - epochs_ : 0;
+    const std::string tmp = path + ".tmp";
+    {
+        std::ofstream out(tmp, std::ios::binary | std::ios::trunc);
+        if (!out) throw WlgError(WLG_ERR_IO, "Cannot write run checkpoint " + tmp);
+        put_raw(out, &hd, 1);
+        put_raw(out, win_.data(), win_.size());
+        put_raw(out, &ctl, 1);
+        put_raw(out, &rep, 1);
+        for (size_t w = 0; w < W; ++w) {
+            put_raw(out, &st[w], 1);
+            put_raw(out, spins.data() + static_cast<size_t>(st[w].slot) * ld, ld);
+            put_raw(out, fields.data() + static_cast<size_t>(st[w].slot) * ld, ld);
+        }
+        put_raw(out, lg.data(), WB);
+        put_raw(out, h.data(), WB);
+        put_raw(out, act.data(), WB);
+        if (features_) {
+            put_raw(out, ref.data(), WB);
+            put_raw(out, sq.data(), WB);
+            put_raw(out, ds.data(), WB);
+        }
+        if (R) {
+            put_raw(out, re.data(), R);
+            put_raw(out, rd.data(), R);
+            put_raw(out, rt.data(), R);
+            put_raw(out, rp.data(), R);
+            put_raw(out, rs.data(), R * ld);
+        }
+        out.flush();
+        if (!out) throw WlgError(WLG_ERR_IO, "Cannot write run checkpoint " + tmp);
+    }
+    if (std::rename(tmp.c_str(), path.c_str()) != 0) throw WlgError(WLG_ERR_IO, "Cannot replace " + path);
+}
+
+void Engine::load_run(const std::string& path) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in) throw WlgError(WLG_ERR_IO, "Cannot open run checkpoint " + path);
+    const size_t W = walkers_, B = bins_, ld = sys_.ld, WB = W * B;
+    const size_t R = p_.collect ? W * kRepresentatives : 0;
+    RunHeader hd{};
+    get_raw(in, &hd, 1);
+    if (std::memcmp(hd.magic, kRunMagic, 8) != 0) throw WlgError(WLG_ERR_IO, "Not a run checkpoint");
+    if (hd.walkers != W || hd.windows != windows_ || hd.n != sys_.n || hd.ld != ld || hd.bins != B ||
+        hd.system_hash != system_hash_ || hd.precision != precision_ || hd.features != (features_ ? 1 : 0) ||
+        hd.collect != (p_.collect ? 1 : 0) || hd.emin != cfg_.emin || hd.emax != cfg_.emax ||
+        hd.width != cfg_.bin_width)
+        throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Run checkpoint is incompatible with this run");
+    std::vector<uint64_t> win(win_.size());
+    get_raw(in, win.data(), win.size());
+    if (win != win_) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Run checkpoint has other energy windows");
+    Control ctl{};
+    PrecisionReport rep{};
+    get_raw(in, &ctl, 1);
+    get_raw(in, &rep, 1);
+    std::vector<WalkerState> st(W);
+    std::vector<int8_t> spins(W * ld);
+    std::vector<double> fields(W * ld);
+    for (size_t w = 0; w < W; ++w) {
+        get_raw(in, &st[w], 1);
+        get_raw(in, spins.data() + w * ld, ld);
+        get_raw(in, fields.data() + w * ld, ld);
+        st[w].slot = static_cast<int32_t>(w);
+        if (st[w].window != static_cast<int32_t>(w / wpw_))
+            throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Run checkpoint walker order mismatch");
+    }
+    std::vector<double> lg(WB);
+    std::vector<uint64_t> h(WB);
+    std::vector<uint8_t> act(WB);
+    get_raw(in, lg.data(), WB);
+    get_raw(in, h.data(), WB);
+    get_raw(in, act.data(), WB);
+    std::vector<uint8_t> ref;
+    std::vector<double> sq;
+    std::vector<uint64_t> ds;
+    if (features_) {
+        ref.resize(WB);
+        sq.resize(WB);
+        ds.resize(WB);
+        get_raw(in, ref.data(), WB);
+        get_raw(in, sq.data(), WB);
+        get_raw(in, ds.data(), WB);
+    }
+    std::vector<double> re(R), rd(R), rt(R);
+    std::vector<uint8_t> rp(R);
+    std::vector<int8_t> rs(R * ld);
+    if (R) {
+        get_raw(in, re.data(), R);
+        get_raw(in, rd.data(), R);
+        get_raw(in, rt.data(), R);
+        get_raw(in, rp.data(), R);
+        get_raw(in, rs.data(), R * ld);
+    }
+    check_cuda(cudaMemcpyAsync(d_ctl_.ptr, &ctl, sizeof ctl, cudaMemcpyHostToDevice, stream_), "copy control");
+    check_cuda(cudaMemcpyAsync(d_prec_.ptr, &rep, sizeof rep, cudaMemcpyHostToDevice, stream_), "copy report");
+    upload(d_ws_, st, stream_);
+    upload(d_spins_, spins, stream_);
+    upload(d_fields_, fields, stream_);
+    upload(d_log_g_, lg, stream_);
+    upload(d_hist_, h, stream_);
+    upload(d_active_, act, stream_);
+    if (features_) {
+        upload(d_refine_, ref, stream_);
+        upload(d_sqdisp_, sq, stream_);
+        upload(d_dsamples_, ds, stream_);
+    }
+    if (R) {
+        upload(d_rep_energy_, re, stream_);
+        upload(d_rep_dist_, rd, stream_);
+        upload(d_rep_target_, rt, stream_);
+        upload(d_rep_present_, rp, stream_);
+        upload(d_rep_spins_, rs, stream_);
+    }
+    check_cuda(cudaStreamSynchronize(stream_), "restore");
+    done_ = ctl.done != 0;
+    epochs_ = ctl.epoch;
+    recomputes_ = hd.recomputes;
+    if (recompute_epochs_) next_recompute_ = epochs_ + hd.next_recompute_in;
+    last_checkpoint_ = st[0].attempted;
 }
 
 }  // namespace wlg

@@ -244,6 +244,10 @@ class Engine {
     void swap(uint64_t left, uint64_t right);
     void precision_report(wlg_precision_report* out);
     void warm_start(const double* log_g, double factor);
+    // every walker's state, the control block and the recompute schedule (multi-walker
+    // checkpoint; the reference checkpoints single-walker runs only)
+    void save_run(const std::string& path);
+    void load_run(const std::string& path);
     // batch support: the captured epoch graph (built on first use, after one direct epoch that
     // primes the kernels) and the host work after epochs that a batch launch ran
     cudaGraph_t epoch_graph();
@@ -295,6 +299,8 @@ class Engine {
     uint64_t last_checkpoint_ = 0;
     bool done_ = false;
     bool finished_ = false;
+    bool checkpointing_all_ = false;  // more than one walker: the multi-walker format
+    uint64_t system_hash_ = 0;
     uint64_t epochs_ = 0;
     double next_progress_ = 0.0;
     size_t progress_width_ = 0;

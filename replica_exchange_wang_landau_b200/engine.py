@@ -550,6 +550,14 @@ class Engine:
         _check(self._lib.wlg_engine_time_run(self._h, int(epochs), C.byref(t)))
         return {name: getattr(t, name) for name, _ in _abi.wlg_epoch_timing._fields_}
 
+    def save_run(self, path: str) -> None:
+        """Checkpoint of every walker and the run counters (no reference counterpart)."""
+        _check(self._lib.wlg_engine_save_run(self._h, str(path).encode()))
+
+    def load_run(self, path: str) -> None:
+        """Restores a save_run checkpoint into this compatible engine."""
+        _check(self._lib.wlg_engine_load_run(self._h, str(path).encode()))
+
     def autotune(self, trial_epochs: int = 16) -> dict:
         """Times candidate launch shapes on real epochs and keeps the fastest (results are
         unchanged by the launch shape)."""
