@@ -391,6 +391,39 @@ wlg_status wlg_write_fragment_csv(const char* path, double emin, double width, u
                                   uint64_t window_begin, uint64_t window_end, const double* log_g,
                                   const uint64_t* histogram, const double* standard_error, const uint8_t* valid);
 
+/* ---- the adaptive-window pilot (apps/wl_run.cpp:104-169; src/analysis.cpp:183-420) ------ */
+/* wl::AdaptiveWindowParameters (include/wl/analysis.hpp:28-38). */
+typedef struct wlg_adaptive_parameters {
+    uint64_t iterations;                /* pilot rounds (2)                                   */
+    double pilot_mcs;                   /* MCS per pilot round (10000)                        */
+    double smoothing_width;             /* energy units; 0 = automatic                        */
+    double minimum_width;               /* energy units; 0 = a quarter of the mean core width */
+    double diffusivity_floor_fraction;  /* 0.05                                               */
+    double curvature_weight;            /* 0.25                                               */
+    double round_trip_target;           /* 2                                                  */
+    double maximum_round_trip_penalty;  /* 3                                                  */
+} wlg_adaptive_parameters;
+/* One window's pilot sampling statistics (wl::WindowSamplingStatistics), whole-grid arrays. */
+typedef struct wlg_sampling_view {
+    uint64_t window_begin, window_end;
+    const double* squared_energy_displacement;
+    const uint64_t* displacement_samples;
+    uint64_t round_trips;
+    uint64_t walkers;
+} wlg_sampling_view;
+/* adapt_energy_windows (src/analysis.cpp:183-339): windows_out gets 2*count (begin, end). */
+wlg_status wlg_adapt_energy_windows(double emin, double emax, double width, const wlg_fragment_view* fragments,
+                                    const wlg_sampling_view* sampling, uint64_t count, double overlap,
+                                    const wlg_adaptive_parameters* parameters, uint64_t* windows_out);
+/* select_adaptive_initial_configurations (src/analysis.cpp:341-420), one process: seeds for
+ * count*walkers_per_window walkers (spins_out row-major, present_out 0 where none). */
+wlg_status wlg_select_initial_configurations(double emin, double emax, double width, const uint64_t* windows,
+                                             uint64_t count, const double* representative_energy,
+                                             const int8_t* representative_spins, const uint8_t* representative_present,
+                                             uint64_t representatives, uint64_t spins, uint64_t walkers_per_window,
+                                             int8_t* spins_out, uint8_t* present_out, uint64_t* missing,
+                                             uint64_t* external);
+
 /* ---- batches of engines (no counterpart in the reference, which runs one instance) -----
  * Engines created on the same device (different systems, sizes, windows or precisions)
  * advanced together: one CUDA graph whose child graphs are the engines' captured epoch

@@ -268,6 +268,8 @@ class Reference(_Checker):
                                          P(_u64), P(_dbl), P(C.c_uint8), P(_u64), C.c_char_p, _cp, _sz]),
             "ref_write_fragment_csv": (C.c_int, [C.c_char_p, _dbl, _dbl, _dbl, P(_abi.wlg_fragment_view), _u64, _cp,
                                                  _sz]),
+            "ref_select_initial": (C.c_int, [_vp, _dbl, _dbl, _dbl, P(_u64), _u64, _u64, _u64, P(C.c_int8),
+                                             P(C.c_uint8), P(_u64), P(_u64), _cp, _sz]),
         }
         for name, (res, args) in sig.items():
             getattr(L, name).restype = res
@@ -275,6 +277,10 @@ class Reference(_Checker):
 
     def set_threads(self, threads: int) -> int:
         return int(self.lib.ref_set_threads(int(threads)))
+
+    def pilot_round(self, system: System, config: RunConfig):
+        """(result, adapted windows, seeds per walker, missing, external) of one reference round."""
+        return _pilot_round(self, system, config)
 
     def stitch_dos(self, views, emin, emax, width, complete_range: bool, spins: int, dos_csv: str = ""):
         """wl::stitch_dos on wlg_fragment_view inputs; also writes <dos_csv> when given."""
@@ -343,6 +349,36 @@ class Reference(_Checker):
             return _collect_result(self.lib, "ref", r, system.size(), config)
         finally:
             self.lib.ref_result_destroy(r)
+
+
+def _pilot_round(ref: "Reference", system: System, config: RunConfig):
+    """One adaptive-window round of the reference: run_rewl with pilot statistics, then its
+    adapt_energy_windows and select_adaptive_initial_configurations on that result."""
+    c, keep = config._struct(system.size())
+    err = _err()
+    lib = ref.lib
+    r = lib.ref_run_rewl(C.byref(system._struct()), C.byref(c), err, len(err))
+    if not r:
+        raise CheckerError(6, err.value.decode())
+    try:
+        result = _collect_result(lib, "ref", r, system.size(), config)
+        count = int(config.windows)
+        w = np.zeros(2 * count, np.uint64)
+        _raise(lib.ref_adapt_windows(r, config.emin, config.emax, config.bin_width, count, config.overlap,
+                                     _u64ptr(w), err, len(err)), err)
+        n = system.size()
+        total = count * int(config.walkers)
+        spins = np.zeros((total, n), np.int8)
+        present = np.zeros(total, np.uint8)
+        missing, external = C.c_uint64(0), C.c_uint64(0)
+        _raise(lib.ref_select_initial(r, config.emin, config.emax, config.bin_width, _u64ptr(w), count,
+                                      int(config.walkers), n, _i8ptr(spins), _u8ptr(present), C.byref(missing),
+                                      C.byref(external), err, len(err)), err)
+        windows = [(int(w[2 * k]), int(w[2 * k + 1])) for k in range(count)]
+        seeds = [spins[k].copy() if present[k] else None for k in range(total)]
+        return result, windows, seeds, int(missing.value), int(external.value)
+    finally:
+        lib.ref_result_destroy(r)
 
 
 def _collect_result(lib, prefix, r, n, config: RunConfig) -> RewlResult:

@@ -443,4 +443,24 @@ int ref_write_fragment_csv(const char* path, double emin, double emax, double wi
     } catch (const std::exception& e) { put_error(err, errlen, e.what()); return status_of(e); }
 }
 
+int ref_select_initial(void* handle, double emin, double emax, double width, const uint64_t* windows, uint64_t count,
+                       uint64_t walkers, uint64_t n, int8_t* spins_out, uint8_t* present_out, uint64_t* missing,
+                       uint64_t* external, char* err, size_t errlen) {
+    try {
+        const auto& r = static_cast<ResultHandle*>(handle)->result;
+        std::vector<wl::EnergyWindow> w(count);
+        for (uint64_t k = 0; k < count; ++k) w[k] = {windows[2 * k], windows[2 * k + 1]};
+        std::size_t miss = 0, ext = 0;
+        const auto seeds = wl::select_adaptive_initial_configurations({emin, emax, width}, w, r.representatives, 1,
+                                                                      walkers, miss, ext);
+        for (std::size_t k = 0; k < seeds.size(); ++k) {
+            present_out[k] = seeds[k].empty() ? 0 : 1;
+            if (!seeds[k].empty()) std::copy(seeds[k].begin(), seeds[k].end(), spins_out + k * n);
+        }
+        *missing = miss;
+        *external = ext;
+        return 0;
+    } catch (const std::exception& e) { put_error(err, errlen, e.what()); return status_of(e); }
+}
+
 } // extern "C"

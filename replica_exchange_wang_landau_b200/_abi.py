@@ -181,6 +181,30 @@ class wlg_join_quality(C.Structure):
     ]
 
 
+class wlg_adaptive_parameters(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_uint64),
+        ("pilot_mcs", C.c_double),
+        ("smoothing_width", C.c_double),
+        ("minimum_width", C.c_double),
+        ("diffusivity_floor_fraction", C.c_double),
+        ("curvature_weight", C.c_double),
+        ("round_trip_target", C.c_double),
+        ("maximum_round_trip_penalty", C.c_double),
+    ]
+
+
+class wlg_sampling_view(C.Structure):
+    _fields_ = [
+        ("window_begin", C.c_uint64),
+        ("window_end", C.c_uint64),
+        ("squared_energy_displacement", C.POINTER(C.c_double)),
+        ("displacement_samples", C.POINTER(C.c_uint64)),
+        ("round_trips", C.c_uint64),
+        ("walkers", C.c_uint64),
+    ]
+
+
 class wlg_snapshot(C.Structure):
     _fields_ = [
         ("walker_id", C.c_uint64),
@@ -213,6 +237,8 @@ STRUCTS = {
     "wlg_autotune_report": wlg_autotune_report,
     "wlg_fragment_view": wlg_fragment_view,
     "wlg_join_quality": wlg_join_quality,
+    "wlg_adaptive_parameters": wlg_adaptive_parameters,
+    "wlg_sampling_view": wlg_sampling_view,
 }
 
 P = C.POINTER
@@ -252,6 +278,11 @@ SIGNATURES = {
     "wlg_write_dos_csv": (_i32, [C.c_char_p, _dbl, _dbl, _u64, P(_dbl), P(_u64), P(_dbl), P(C.c_uint8)]),
     "wlg_write_fragment_csv": (_i32, [C.c_char_p, _dbl, _dbl, _u64, _u64, _u64, P(_dbl), P(_u64), P(_dbl),
                                       P(C.c_uint8)]),
+    "wlg_adapt_energy_windows": (_i32, [_dbl, _dbl, _dbl, P(wlg_fragment_view), P(wlg_sampling_view), _u64, _dbl,
+                                        P(wlg_adaptive_parameters), P(_u64)]),
+    "wlg_select_initial_configurations": (_i32, [_dbl, _dbl, _dbl, P(_u64), _u64, P(_dbl), P(C.c_int8),
+                                                 P(C.c_uint8), _u64, _u64, _u64, P(C.c_int8), P(C.c_uint8), P(_u64),
+                                                 P(_u64)]),
     "wlg_batch_create": (_i32, [P(_vp), _u64, P(_vp)]),
     "wlg_batch_run_epochs": (_i32, [_vp, _u64, P(_u64), P(_i32)]),
     "wlg_batch_destroy": (None, [_vp]),

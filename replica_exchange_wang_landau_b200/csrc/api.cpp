@@ -600,4 +600,30 @@ wlg_status wlg_write_fragment_csv(const char* path, double emin, double width, u
     });
 }
 
+// ---- the adaptive-window pilot's host steps ------------------------------------------
+
+wlg_status wlg_adapt_energy_windows(double emin, double emax, double width, const wlg_fragment_view* fragments,
+                                    const wlg_sampling_view* sampling, uint64_t count, double overlap,
+                                    const wlg_adaptive_parameters* parameters, uint64_t* windows_out) {
+    return guarded([&] {
+        if (!parameters || !windows_out) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        const auto w = wlg::adapt_energy_windows(emin, emax, width, fragments, sampling, count, overlap, *parameters);
+        std::copy(w.begin(), w.end(), windows_out);
+    });
+}
+
+wlg_status wlg_select_initial_configurations(double emin, double emax, double width, const uint64_t* windows,
+                                             uint64_t count, const double* representative_energy,
+                                             const int8_t* representative_spins, const uint8_t* representative_present,
+                                             uint64_t representatives, uint64_t spins, uint64_t walkers_per_window,
+                                             int8_t* spins_out, uint8_t* present_out, uint64_t* missing,
+                                             uint64_t* external) {
+    return guarded([&] {
+        if (!spins_out || !present_out) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        wlg::select_initial_configurations(emin, emax, width, windows, count, representative_energy,
+                                           representative_spins, representative_present, representatives, spins,
+                                           walkers_per_window, spins_out, present_out, missing, external);
+    });
+}
+
 }  // extern "C"

@@ -97,6 +97,15 @@ bool load_checkpoint_file(const std::string& path, std::vector<int8_t>& spins, s
                           std::vector<double>& log_g, std::vector<uint64_t>& hist, std::vector<uint8_t>& active,
                           wlg_snapshot& scalars, std::string& error);
 
+// adaptive.cpp
+std::vector<uint64_t> adapt_energy_windows(double emin, double emax, double width, const wlg_fragment_view* fragments,
+                                           const wlg_sampling_view* sampling, uint64_t count, double overlap,
+                                           const wlg_adaptive_parameters& p);
+void select_initial_configurations(double emin, double emax, double width, const uint64_t* windows, uint64_t count,
+                                   const double* rep_energy, const int8_t* rep_spins, const uint8_t* rep_present,
+                                   uint64_t reps, uint64_t n, uint64_t walkers_per_window, int8_t* spins_out,
+                                   uint8_t* present_out, uint64_t* missing, uint64_t* external);
+
 // stitch.cpp
 void stitch_dos(double emin, double emax, double width, const wlg_fragment_view* fragments, uint64_t count,
                 bool complete_range, uint64_t spins, double* log_g, uint64_t* histogram, double* standard_error,

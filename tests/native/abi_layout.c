@@ -55,6 +55,13 @@ int main(void) {
     F(wlg_fragment_view, valid);
     S(wlg_join_quality); F(wlg_join_quality, join_bin); F(wlg_join_quality, common_bins); F(wlg_join_quality, rmse);
     F(wlg_join_quality, max_abs_difference); F(wlg_join_quality, slope_difference);
+    S(wlg_adaptive_parameters); F(wlg_adaptive_parameters, iterations); F(wlg_adaptive_parameters, pilot_mcs);
+    F(wlg_adaptive_parameters, smoothing_width); F(wlg_adaptive_parameters, minimum_width);
+    F(wlg_adaptive_parameters, diffusivity_floor_fraction); F(wlg_adaptive_parameters, curvature_weight);
+    F(wlg_adaptive_parameters, round_trip_target); F(wlg_adaptive_parameters, maximum_round_trip_penalty);
+    S(wlg_sampling_view); F(wlg_sampling_view, window_begin); F(wlg_sampling_view, window_end);
+    F(wlg_sampling_view, squared_energy_displacement); F(wlg_sampling_view, displacement_samples);
+    F(wlg_sampling_view, round_trips); F(wlg_sampling_view, walkers);
     S(wlg_snapshot); F(wlg_snapshot, walker_id); F(wlg_snapshot, spins); F(wlg_snapshot, fields);
     F(wlg_snapshot, energy); F(wlg_snapshot, log_g); F(wlg_snapshot, histogram); F(wlg_snapshot, active);
     F(wlg_snapshot, factor); F(wlg_snapshot, attempted); F(wlg_snapshot, accepted); F(wlg_snapshot, forced_accepted);
