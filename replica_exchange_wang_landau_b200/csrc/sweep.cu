@@ -521,6 +521,16 @@ __device__ __forceinline__ uint32_t ld_acquire_shared(uint32_t addr) {
     asm volatile("ld.acquire.cta.shared::cta.u32 %0, [%1];" : "=r"(value) : "r"(addr) : "memory");
     return value;
 }
+// Non-blocking test of the completion of phase `parity` of one barrier.
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
 // Bounded wait of one thread for the completion of phase `parity` of one barrier.
 __device__ __forceinline__ bool mbar_wait_thread(uint32_t bar, uint32_t parity) {
     for (uint32_t k = 0; k < kWaitPolls; ++k)
@@ -776,6 +786,11 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
                 failed = true;
                 break;
             }
+            // Look ahead at the next batch without blocking; the result is used at the end
+            // of the attempt, so the test's latency overlaps the chain.  Every batch before
+            // ready_to has completed, so that batch's barrier is in its phase or past it.
+            const uint32_t next_batch = ready_to >> 2;
+            const bool next_ready = mbar_test(bar_addr + 8 * (next_batch & bm), (next_batch >> blog) & 1u);
             const JT* prow = ring + static_cast<size_t>(prev_slot) * row_stride;
             if (i < 0) {  // rare: bounded() rejects draw hq; the next draw is the candidate site
                 hq += 1;
@@ -801,6 +816,20 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
             const double r1 = coupling<kPrec>(row, c1l), r2 = coupling<kPrec>(row, c2l);
             const double p1 = coupling<kPrec>(prow, c1l), p2 = coupling<kPrec>(prow, c2l);
             const double rscale = kPrec == WLG_PRECISION_BF16 ? rec_rs[slot] : 1.0;
+            const double fc1 = fma(m_prev, p1, f1), fc2 = fma(m_prev, p2, f2);
+
+            // the decision (attempt_flip, src/wang_landau.cpp:244-262)
+            const double m = si > 0 ? -2.0 : 2.0;  // -2 * spin
+            const double Ep = fma(m, h, E);
+            const bool in_range = Ep >= g.minimum && Ep <= g.maximum;
+            const double qv = kPow2 ? fma(Ep, g.inv_width, neg_min_scaled) : (Ep - g.minimum) / g.width;
+            int nb = in_range ? __double2int_rd(qv) : -1;
+            nb = (nb == gcount && Ep == g.maximum) ? gcount - 1 : nb;
+            const bool in_window = nb >= wb && nb < we;
+            const double lg_load = lg_s[in_window ? nb - wb : 0];
+            // The row of the previous attempt is read only now: its 16-byte loads, issued
+            // earlier, would queue ahead of the log g load on the chain.
+            asm volatile("" ::: "memory");
             double2 rb[kChunks];
 #pragma unroll
             for (int k = 0; k < kChunks; ++k) {
@@ -813,17 +842,6 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
                 fr[k].x = fma(m_prev, rb[k].x, fr[k].x);
                 fr[k].y = fma(m_prev, rb[k].y, fr[k].y);
             }
-            const double fc1 = fma(m_prev, p1, f1), fc2 = fma(m_prev, p2, f2);
-
-            // the decision (attempt_flip, src/wang_landau.cpp:244-262)
-            const double m = si > 0 ? -2.0 : 2.0;  // -2 * spin
-            const double Ep = fma(m, h, E);
-            const bool in_range = Ep >= g.minimum && Ep <= g.maximum;
-            const double qv = kPow2 ? fma(Ep, g.inv_width, neg_min_scaled) : (Ep - g.minimum) / g.width;
-            int nb = in_range ? __double2int_rd(qv) : -1;
-            nb = (nb == gcount && Ep == g.maximum) ? gcount - 1 : nb;
-            const bool in_window = nb >= wb && nb < we;
-            const double lg_load = lg_s[in_window ? nb - wb : 0];
             const double lg_new = nb == cur ? lg_cur : lg_load;
             const double log_ratio = lg_cur - lg_new;
             const bool det = log_ratio >= 0.0;
@@ -889,6 +907,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
             lnu = need_u ? l3 : l2;
             m_prev = m_eff;
             prev_slot = slot;
+            ready_to += __all_sync(kFull, next_ready) ? static_cast<uint32_t>(kDrawBatch) : 0u;
         }
     };
     if (!failed) {
