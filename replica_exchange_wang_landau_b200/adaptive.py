@@ -116,10 +116,12 @@ def adaptive_pilot(system: System, config: RunConfig, params: AdaptiveParameters
                                        float(config.overlap), params)
         initial, missing, external = select_initial_configurations(
             config.emin, config.emax, config.bin_width, windows, result.representatives, n, int(config.walkers))
-        if log:
+        if log:  # the line wl_run prints (apps/wl_run.cpp:133-160), default stream formatting
             trips = sum(s.round_trips for s in result.sampling_statistics)
-            ranges = ";".join(f"[{config.emin + b * config.bin_width:.17g},{config.emin + e * config.bin_width:.17g})"
+            seeded = [e for e, s in result.representatives if s is not None and len(s)]
+            lowest = f" minimum_seed_energy={min(seeded):g}" if seeded else ""
+            ranges = ";".join(f"[{config.emin + b * config.bin_width:g},{config.emin + e * config.bin_width:g})"
                               for b, e in windows)
             log(f"adaptive_window_round_trips={trips} seeded_walkers={len(initial) - missing}/{len(initial)} "
-                f"external_warm_starts={external} energy_ranges={ranges}")
+                f"external_warm_starts={external}{lowest} energy_ranges={ranges}")
     return windows, initial
