@@ -468,7 +468,12 @@ def main() -> None:
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-extras", action="store_true",
                     help="skip the mixed-precision lines and the learned-vs-plain time to accuracy")
+    ap.add_argument("--csr-only", action="store_true",
+                    help="print only the CSR configuration's line (the 32^3 lattice, 1024 walkers)")
     args = ap.parse_args()
+    if args.csr_only:
+        print(json.dumps({"csr_batched": csr_batched_line()}))
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

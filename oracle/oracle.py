@@ -114,6 +114,7 @@ class Oracle(_Checker):
             "orc_couplings_destroy": (None, [_vp]),
             "orc_couplings_size": (_u64, [_vp]),
             "orc_couplings_nnz": (_u64, [_vp]),
+            "orc_couplings_set_update_fp32": (None, [_vp, C.c_int]),
             "orc_couplings_dense": (None, [_vp, P(_dbl)]),
             "orc_local_fields": (None, [_vp, P(C.c_int8), P(_dbl)]),
             "orc_total_energy": (_dbl, [_vp, P(C.c_int8)]),
@@ -456,6 +457,12 @@ class CheckerWalker:
 
     def _fn(self, name):
         return getattr(self.L, f"{self.p}_{name}")
+
+    def set_update_fp32(self, on: bool = True):
+        """Follow an FP32 engine walker from here on: flips add m * float(J) (restatement only)."""
+        if self.p != "orc":
+            raise CheckerError(1, "only the restatement has the FP32 update")
+        self.L.orc_couplings_set_update_fp32(self._coup, 1 if on else 0)
 
     def run_attempts(self, count: int):
         err = _err()

@@ -107,6 +107,7 @@ struct orc_couplings {
     uint64_t* offsets; /* CSR: n+1                                       */
     uint64_t* columns; /* CSR: nnz                                       */
     double* values;    /* CSR: nnz                                       */
+    int update_fp32;   /* add_flip_delta with FP32-rounded couplings      */
 };
 
 /* Geometry::validate (physics.cpp:34-56) */
@@ -252,16 +253,20 @@ double orc_total_energy(const orc_couplings* c, const int8_t* spins) {
 }
 
 /* add_flip_delta (physics.cpp:190-195, 231-236) */
+static double update_value(const orc_couplings* c, double v) { return c->update_fp32 ? (double)(float)v : v; }
+
 static void add_flip_delta(const orc_couplings* c, uint64_t flipped, int8_t old_spin, double* fields) {
     const double multiplier = -2.0 * (double)old_spin;
     const uint64_t n = c->n;
     if (!c->csr) {
-        for (uint64_t j = 0; j < n; ++j) fields[j] += multiplier * c->dense[j * n + flipped];
+        for (uint64_t j = 0; j < n; ++j) fields[j] += multiplier * update_value(c, c->dense[j * n + flipped]);
     } else {
         for (uint64_t k = c->offsets[flipped]; k < c->offsets[flipped + 1]; ++k)
-            fields[c->columns[k]] += multiplier * c->values[k];
+            fields[c->columns[k]] += multiplier * update_value(c, c->values[k]);
     }
 }
+
+void orc_couplings_set_update_fp32(orc_couplings* c, int on) { c->update_fp32 = on != 0; }
 
 /* ---- energy grid and windows (src/wang_landau.cpp:13-61) ---------------------- */
 

@@ -27,6 +27,11 @@ orc_couplings* orc_couplings_create(const wlg_system* s, char* err, size_t errle
 void orc_couplings_destroy(orc_couplings* c);
 uint64_t orc_couplings_size(const orc_couplings* c);
 uint64_t orc_couplings_nnz(const orc_couplings* c);
+/* Not in the reference: the update arithmetic of the engine's FP32 runs.  With on != 0,
+ * add_flip_delta adds m * (double)(float)J instead of m * J; local fields and energies stay
+ * FP64.  Set it after a walker's construction to follow an FP32 engine walker, whose
+ * initialisation uses the FP64 couplings. */
+void orc_couplings_set_update_fp32(orc_couplings* c, int on);
 void orc_couplings_dense(const orc_couplings* c, double* out);
 void orc_local_fields(const orc_couplings* c, const int8_t* spins, double* fields);
 double orc_total_energy(const orc_couplings* c, const int8_t* spins);

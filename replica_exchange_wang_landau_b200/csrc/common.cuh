@@ -299,6 +299,10 @@ struct EngineView {
     const int32_t* csr_col;
     const double* csr_val64;
     const float* csr_val32;
+    const int32_t* ell_col;        // ELLPACK copy of the CSR rows: n x ell_width, column -1 pads
+    const double* ell_val64;       // FP64 couplings (FP64 runs)
+    const float* ell_val32;        // FP32 couplings (FP32 runs)
+    int32_t ell_width;             // 32, 64, 128 or 256; 0 when not built
     Grid grid;
     int32_t walkers;
     int32_t walkers_per_window;

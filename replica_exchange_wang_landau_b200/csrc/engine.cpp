@@ -227,6 +227,10 @@ void Engine::initialise_walkers(const wlg_run_config& c) {
     v.csr_col = sys_.csr_col.get<int32_t>();
     v.csr_val64 = sys_.csr_val64.get<double>();
     v.csr_val32 = sys_.csr_val32.get<float>();
+    v.ell_col = sys_.ell_col.get<int32_t>();
+    v.ell_val64 = sys_.ell_val64.get<double>();
+    v.ell_val32 = sys_.ell_val32.get<float>();
+    v.ell_width = sys_.ell_width;
     v.grid = grid_;
     v.walkers = static_cast<int32_t>(W);
     v.walkers_per_window = static_cast<int32_t>(wpw_);

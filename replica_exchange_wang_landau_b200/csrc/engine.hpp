@@ -84,6 +84,8 @@ struct DeviceSystem {
     DeviceBuffer pos, axes;
     DeviceBuffer J64, J32, J16, Jscale;
     DeviceBuffer csr_ptr, csr_col, csr_val64, csr_val32;
+    DeviceBuffer ell_col, ell_val64, ell_val32;  // ELLPACK rows for the CSR sweep
+    int32_t ell_width = 0;                       // entries per row (0: not built)
 };
 
 // Host-side validation and helpers (host.cpp).
@@ -173,6 +175,9 @@ void launch_init(const EngineView& v, const InitArgs& a, int walkers_per_block, 
 void launch_walk(const EngineView& v, const WalkArgs& a, int walkers_per_block, cudaStream_t stream);
 // sweep.cu: the dense sweep; false when the walker does not fit the shared-memory ring.
 bool launch_sweep_dense(const EngineView& v, const WalkArgs& a, cudaStream_t stream);
+bool launch_sweep_csr(const EngineView& v, const WalkArgs& a, int walkers_per_block, cudaStream_t stream);
+void launch_ell_fill(int n, int width, const int32_t* ptr, const int32_t* col, const double* val64,
+                     const float* val32, int32_t* ell_col, double* ell_val64, float* ell_val32, cudaStream_t stream);
 void launch_exchange(const EngineView& v, cudaStream_t stream);
 // precision.cu: drift measurement and resync after an FP64 recompute of all fields.
 void launch_resync(const EngineView& v, const double* rfields, const double* renergy, PrecisionReport* report,

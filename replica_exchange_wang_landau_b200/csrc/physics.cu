@@ -260,6 +260,21 @@ void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream) {
                                                                      d.csr_val64.get<double>(),
                                                                      d.csr_val32.get<float>());
         check_cuda(cudaGetLastError(), "csr_fill_kernel");
+        // the ELLPACK copy read by the CSR sweep (rows of at most 256 couplings)
+        int32_t zmax = 0;
+        for (int32_t c : host_counts) zmax = std::max(zmax, c);
+        int32_t width = 32;
+        while (width < zmax && width < 256) width *= 2;
+        if (zmax <= 256) {
+            const size_t entries = static_cast<size_t>(n) * static_cast<size_t>(width);
+            d.ell_col.allocate(entries * sizeof(int32_t));
+            if (precision == WLG_PRECISION_FP32) d.ell_val32.allocate(entries * sizeof(float));
+            else d.ell_val64.allocate(entries * sizeof(double));
+            launch_ell_fill(n, width, d.csr_ptr.get<int32_t>(), d.csr_col.get<int32_t>(), d.csr_val64.get<double>(),
+                            d.csr_val32.get<float>(), d.ell_col.get<int32_t>(), d.ell_val64.get<double>(),
+                            d.ell_val32.get<float>(), stream);
+            d.ell_width = width;
+        }
     }
     int host_err = 0;
     check_cuda(cudaMemcpyAsync(&host_err, err.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream), "copy err");

@@ -1,0 +1,433 @@
+// sweep_csr.cu — the REWL sweep for cutoff (CSR) couplings: WangLandauWalker::run_attempts /
+// attempt_flip (src/wang_landau.cpp:244-315) with CsrCouplings::add_flip_delta
+// (src/physics.cpp:231-236) for one batch of exchange_interval attempts, then the
+// walker-local flatness / 1/t check of run_rewl (src/parallel.cpp:395-407).
+//
+// Large cutoff systems (a 32^3 lattice: 256 KB of FP64 fields and 32 KB of spins per walker,
+// a thousand walkers) keep each walker's fields and spins in HBM; only the window slice of
+// log g / H / visited lives in shared memory (a few KB), so every walker of a run is resident
+// at once.  An attempt is then bound by memory latency, and the kernel is arranged so that an
+// attempt waits for about one round trip:
+//
+// * The couplings are laid out as ELLPACK rows of 32*K entries (K = 1, 2, 4, 8; column -1 and
+//   value 0 pad a row) with lane j holding entries j, j+32, ...: one coalesced load per
+//   chunk and no row-pointer indirection.
+// * The site of the next attempt is draw hq+1 or, when this attempt consumes the acceptance
+//   uniform, draw hq+2 (the lookahead of the dense split sweep).  The warp holds both
+//   candidates' field, spin and couplings row in registers, loaded at least one attempt
+//   ahead.  A candidate's field is loaded after the stores of every earlier flip and is
+//   corrected for the flip of the current attempt when the candidate is a neighbour of the
+//   flipped site (a ballot over the flipped row finds J_ic), and its spin when it is the
+//   flipped site, so it equals the reference's field when the candidate becomes the site:
+//   fma(m, J, f) with m = +-2 rounds the reference's f + m*J once.
+// * At the end of an attempt, after its stores, the warp issues the loads of the next site's
+//   neighbour fields (speculatively: a rejected flip discards them) before the next
+//   acceptance log; the next attempt decides and on acceptance stores
+//   fields[c] = fma(m, J_ic, fields[c]) for every neighbour c.  Each field changes at most
+//   once per flip, so the order of the neighbour updates is immaterial.
+// * All 32 lanes evaluate the decision chain redundantly; histogram increments go to a
+//   32-bit shared-memory delta per bin that is folded into H at the end of the batch, and the
+//   Wang-Landau count of active bins is updated once from the visited mask, as in the dense
+//   split sweep.
+// The kernel has no waits on other warps or kernels.  Bit-exactness of the rearranged
+// arithmetic is argued where the dense sweeps use the same forms (E + (-2s)h as fma(m, h, E);
+// the power-of-two bin index as fma(E', 1/width, -min/width); the acceptance test
+// log(max(u, 2^-53)) < log_ratio with the CUDA log).
+#include <type_traits>
+
+#include "engine.hpp"
+#include "walker_dev.cuh"
+
+namespace wlg {
+
+namespace {
+
+struct CsrSweepLayout {
+    size_t log_g, hist, hd, active, total;
+};
+__host__ __device__ inline CsrSweepLayout csr_sweep_layout(int mwb) {
+    CsrSweepLayout L;
+    size_t at = 0;
+    L.log_g = at; at += round16(static_cast<size_t>(mwb) * 8);
+    L.hist = at; at += round16(static_cast<size_t>(mwb) * 8);
+    L.hd = at; at += round16(static_cast<size_t>(mwb) * 4);
+    L.active = at; at += round16(static_cast<size_t>(mwb));
+    L.total = at;
+    return L;
+}
+
+template <int kPrec> struct EllValue { using T = double; };
+template <> struct EllValue<WLG_PRECISION_FP32> { using T = float; };
+
+template <int kPrec>
+__device__ __forceinline__ const typename EllValue<kPrec>::T* ell_values(const EngineView& v) {
+    if constexpr (kPrec == WLG_PRECISION_FP32) return v.ell_val32;
+    else return v.ell_val64;
+}
+
+// One site as the warp holds it: field, spin and this lane's entries of its couplings row.
+template <int kK, class VT>
+struct SiteRegs {
+    int site;  // -1: the draw is rejected by bounded()
+    double f;
+    int s;
+    int col[kK];
+    VT val[kK];
+    double nf[kK];  // the neighbour fields (loaded when the site is next)
+};
+
+template <int kK, bool kPow2, int kPrec>
+__global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArgs a) {
+    using VT = typename EllValue<kPrec>::T;
+    using Site = SiteRegs<kK, VT>;
+    constexpr int kWidth = 32 * kK;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int local = static_cast<int>(blockIdx.x) * static_cast<int>(blockDim.x >> 5) + warp;
+    if (local >= a.count) return;
+    const int w = a.first + local;
+    Control* ctl = v.ctl;
+    if (a.epoch_mode && *reinterpret_cast<volatile int32_t*>(&ctl->done)) return;
+
+    const CsrSweepLayout L = csr_sweep_layout(v.max_window_bins);
+    unsigned char* base = smem + static_cast<size_t>(warp) * L.total;
+    double* lg_s = reinterpret_cast<double*>(base + L.log_g);
+    uint64_t* h_s = reinterpret_cast<uint64_t*>(base + L.hist);
+    uint32_t* hd = reinterpret_cast<uint32_t*>(base + L.hd);
+    uint8_t* act_s = base + L.active;
+
+    WalkerState st = v.ws[w];
+    const int wb = v.win_begin[st.window], we = v.win_end[st.window], nbins = we - wb;
+    if (st.cur_bin < wb || st.cur_bin >= we) {  // "Walker escaped its energy window"
+        if (lane == 0) record_error(ctl, WLG_ERR_ESCAPED, w);
+        return;
+    }
+    const DeviceParams& P = v.p;
+    uint32_t batch;
+    {
+        uint64_t b = a.fixed_batch ? a.fixed_batch : P.exchange_interval;
+        if (!a.fixed_batch && P.max_attempts) {
+            const uint64_t remaining = st.attempted < P.max_attempts ? P.max_attempts - st.attempted : 0;
+            b = remaining < b ? remaining : b;
+        }
+        batch = static_cast<uint32_t>(b < 0xffffffffULL ? b : 0xffffffffULL);
+    }
+    const size_t boff = static_cast<size_t>(w) * static_cast<size_t>(v.grid.count) + static_cast<size_t>(wb);
+    double* fg = v.fields + static_cast<size_t>(st.slot) * v.ld;
+    int8_t* sg = v.spins + static_cast<size_t>(st.slot) * v.ld;
+    const int32_t* __restrict__ ecol = v.ell_col;
+    const VT* __restrict__ evals = ell_values<kPrec>(v);
+    const FastMod fm = v.site_mod;
+
+    for (int b = lane; b < nbins; b += 32) {
+        lg_s[b] = v.log_g[boff + b];
+        h_s[b] = v.hist[boff + b];
+        act_s[b] = v.active[boff + b];
+        hd[b] = 0;
+    }
+    __syncwarp();
+
+    auto site_of = [&](uint64_t d) -> int { return d < fm.threshold ? -1 : static_cast<int>(fast_mod(fm, d)); };
+    // issue the loads of one site's field, spin and row (the field and spin as stored now)
+    auto fetch = [&](int site, Site& c) {
+        c.site = site;
+        const int s = site < 0 ? 0 : site;
+        c.f = fg[s];
+        c.s = sg[s];
+        const size_t r = static_cast<size_t>(s) * kWidth + static_cast<size_t>(lane);
+#pragma unroll
+        for (int k = 0; k < kK; ++k) {
+            c.col[k] = __ldg(ecol + r + 32 * k);
+            c.val[k] = __ldg(evals + r + 32 * k);
+        }
+    };
+    // a candidate after the accepted flip of `flipped` with factor m
+    auto correct = [&](Site& c, const Site& flipped, double m) {
+        bool hit = false;
+        double jv = 0.0;
+#pragma unroll
+        for (int k = 0; k < kK; ++k)
+            if (c.site >= 0 && flipped.col[k] == c.site) {
+                hit = true;
+                jv = static_cast<double>(flipped.val[k]);
+            }
+        const unsigned mask = __ballot_sync(kFull, hit);
+        if (mask) c.f = fma(m, __shfl_sync(kFull, jv, __ffs(mask) - 1), c.f);
+        if (c.site == flipped.site) c.s = -c.s;
+    };
+
+    double E = st.energy;
+    double factor = st.factor;
+    int32_t stage = st.stage;
+    const uint64_t att0 = st.attempted;
+    uint64_t since = st.attempted - st.last_accepted;
+    const uint64_t force_limit = P.force_after != 0 ? P.force_after : ~0ULL;
+    uint32_t n_acc = 0, n_forced = 0;
+    uint64_t active_count = st.active_count;
+    const Grid g = v.grid;
+    const int gcount = static_cast<int>(g.count);
+    const double neg_min_scaled = -g.minimum * g.inv_width;
+    int cur = st.cur_bin;
+    double lg_cur = lg_s[cur - wb];
+    uint64_t active_before = 0;
+    if (stage != kInverseTime) {
+        for (int b = lane; b < nbins; b += 32) active_before += act_s[b] ? 1 : 0;
+        active_before = warp_sum_u64(active_before);
+    }
+
+    // Three register sets hold the site of the next attempt (draw hq) and the candidates
+    // (draws hq+1, hq+2); their roles rotate by one or two places per attempt.  The rotation
+    // is a switch over the three role assignments, not register moves: a move of a set whose
+    // loads are still in flight would wait for them.
+    Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};
+    Site A, B, C;
+    fetch(site_of(rng.next()), A);
+    uint64_t d1 = rng.next(), d2 = rng.next();
+    fetch(site_of(d1), B);
+    fetch(site_of(d2), C);
+    // the neighbour fields of a site, loaded before its attempt (after every earlier store)
+    auto load_neighbours = [&](Site& c) {
+#pragma unroll
+        for (int k = 0; k < kK; ++k) c.nf[k] = c.col[k] >= 0 ? fg[c.col[k]] : 0.0;
+    };
+    load_neighbours(A);
+    double lnu = log(fmax(to_uniform(d1), 0x1.0p-53));
+
+    // The attempts of one batch; kIT selects the 1/t stage (per-attempt factor and active
+    // count) or the Wang-Landau / frozen stages (constant factor).
+    auto run = [&](auto it_tag) {
+        constexpr bool kIT = decltype(it_tag)::value;
+        const bool frozen = stage == kFrozen;
+        double factor_next = factor;
+        if (kIT && active_count != 0) factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + 1);
+        uint32_t t = 0;
+        // One attempt with the roles (site, c1, c2); returns the rotation of the roles.
+        auto attempt = [&](Site& site, Site& c1, Site& c2) -> int {
+            if (site.site < 0) {  // rare: bounded() rejects draw hq; the next draw is the site
+                d1 = d2;
+                d2 = rng.next();
+                fetch(site_of(d2), site);  // becomes c2
+                load_neighbours(c1);
+                lnu = log(fmax(to_uniform(d1), 0x1.0p-53));
+                return 1;
+            }
+            // the decision (attempt_flip, src/wang_landau.cpp:244-262)
+            const double m = site.s > 0 ? -2.0 : 2.0;  // -2 * spin
+            const double Ep = fma(m, site.f, E);
+            const bool in_range = Ep >= g.minimum && Ep <= g.maximum;
+            const double qv = kPow2 ? fma(Ep, g.inv_width, neg_min_scaled) : (Ep - g.minimum) / g.width;
+            int nb = in_range ? __double2int_rd(qv) : -1;
+            nb = (nb == gcount && Ep == g.maximum) ? gcount - 1 : nb;
+            const bool in_window = nb >= wb && nb < we;
+            const double lg_load = lg_s[in_window ? nb - wb : 0];
+            const double lg_new = nb == cur ? lg_cur : lg_load;
+            const double log_ratio = lg_cur - lg_new;
+            const bool det = log_ratio >= 0.0;
+            const bool forced = !det && since >= force_limit;
+            const bool need_u = in_window && !det && !forced;
+            const bool accepted = in_window && (det || forced || lnu < log_ratio);
+
+            if (accepted) {  // add_flip_delta, and the candidates brought up to date
+#pragma unroll
+                for (int k = 0; k < kK; ++k)
+                    if (site.col[k] >= 0) fg[site.col[k]] = fma(m, static_cast<double>(site.val[k]), site.nf[k]);
+                if (lane == 0) sg[site.site] = static_cast<int8_t>(-site.s);
+                correct(c2, site, m);
+                if (!need_u) correct(c1, site, m);  // draw hq+1 becomes the next site
+            }
+            E = accepted ? Ep : E;
+            since = accepted ? 0 : since + 1;
+            n_acc += accepted ? 1u : 0u;
+            n_forced += (accepted && forced) ? 1u : 0u;
+            ++t;
+
+            // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
+            if (kIT && stage == kInverseTime) {
+                factor = factor_next;
+                if (factor <= P.final_factor) stage = kFrozen;
+            }
+            const bool move = accepted && nb != cur;
+            const int ncur = move ? nb : cur;
+            const double lg_base = move ? lg_new : lg_cur;
+            if (kIT) {
+                const bool visited = act_s[ncur - wb] != 0;
+                active_count += visited ? 0 : 1;
+            }
+            if (lane == 0) {
+                lg_s[cur - wb] = lg_cur;
+                atomicAdd(&hd[ncur - wb], 1u);
+                act_s[ncur - wb] = 1;
+            }
+            cur = ncur;
+            if (kIT) {
+                lg_cur = stage != kFrozen ? lg_base + factor : lg_base;
+                if (stage == kInverseTime && active_count != 0)
+                    factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + t + 1);
+            } else {
+                lg_cur = frozen ? lg_base : lg_base + factor;
+            }
+
+            __syncwarp();  // this attempt's stores are visible to every lane before later loads
+            int rotation;
+            if (need_u) {  // draw hq+1 was the uniform: the site is draw hq+2
+                d1 = rng.next();
+                d2 = rng.next();
+                load_neighbours(c2);
+                fetch(site_of(d1), site);  // becomes c1
+                fetch(site_of(d2), c1);    // becomes c2
+                rotation = 2;
+            } else {
+                d1 = d2;
+                d2 = rng.next();
+                load_neighbours(c1);
+                fetch(site_of(d2), site);  // becomes c2
+                rotation = 1;
+            }
+            lnu = log(fmax(to_uniform(d1), 0x1.0p-53));
+            return rotation;
+        };
+        int roles = 0;  // 0: (A, B, C), 1: (B, C, A), 2: (C, A, B)
+        while (t < batch) {
+            int r;
+            if (roles == 0) r = attempt(A, B, C);
+            else if (roles == 1) r = attempt(B, C, A);
+            else r = attempt(C, A, B);
+            roles += r;
+            roles = roles >= 3 ? roles - 3 : roles;
+        }
+    };
+    if (stage == kInverseTime)
+        run(std::true_type{});
+    else
+        run(std::false_type{});
+
+    // the generator is three draws past the last consumed one (the next site, hq+1, hq+2)
+    rng_step_back(rng);
+    rng_step_back(rng);
+    rng_step_back(rng);
+    if (lane == 0) lg_s[cur - wb] = lg_cur;
+    __syncwarp();
+    uint64_t active_after = 0;
+    for (int b = lane; b < nbins; b += 32) {
+        h_s[b] += hd[b];
+        active_after += act_s[b] ? 1 : 0;
+    }
+    active_after = warp_sum_u64(active_after);
+    if (st.stage != kInverseTime) active_count += active_after - active_before;
+    __syncwarp();
+
+    st.rng[0] = rng.s0;
+    st.rng[1] = rng.s1;
+    st.rng[2] = rng.s2;
+    st.rng[3] = rng.s3;
+    st.energy = E;
+    st.factor = factor;
+    st.stage = stage;
+    st.attempted = att0 + batch;
+    st.accepted += n_acc;
+    st.forced += n_forced;
+    st.last_accepted = st.attempted - since;
+    st.active_count = active_count;
+    st.cur_bin = cur;
+
+    if (a.epoch_mode && st.stage == kWangLandau) {
+        const bool at_limit = P.max_attempts != 0 && st.attempted >= P.max_attempts;
+        if (st.attempted - st.last_check >= P.check_interval || at_limit) {
+            st.last_check = st.attempted;
+            const HistStats hs = warp_histogram_statistics(h_s, act_s, nbins, st.active_count, lane);
+            st.last_flatness = P.inverse_time ? hs.coverage : hs.min_over_mean;
+            if (stats_ready(hs, st.stage, P)) warp_begin_next_iteration(st, h_s, nullptr, nbins, P, lane);
+        }
+    }
+    for (int b = lane; b < nbins; b += 32) {
+        v.log_g[boff + b] = lg_s[b];
+        v.hist[boff + b] = h_s[b];
+        v.active[boff + b] = act_s[b];
+    }
+    if (lane == 0) {
+        v.ws[w] = st;
+        if (a.epoch_mode) {
+            if (st.stage == kFrozen) atomicAdd(&ctl->frozen, 1u);
+            if (P.max_attempts != 0 && st.attempted >= P.max_attempts) atomicAdd(&ctl->at_limit, 1u);
+        }
+    }
+}
+
+using SweepFn = void (*)(EngineView, WalkArgs);
+
+template <int kK, bool kPow2, int kPrec>
+SweepFn csr_fn() {
+    static bool configured = false;
+    if (!configured) {
+        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_csr_kernel<kK, kPow2, kPrec>),
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+                   "cudaFuncSetAttribute");
+        configured = true;
+    }
+    return &sweep_csr_kernel<kK, kPow2, kPrec>;
+}
+
+template <bool kPow2, int kPrec>
+SweepFn pick_csr_width(int width) {
+    switch (width) {
+        case 32: return csr_fn<1, kPow2, kPrec>();
+        case 64: return csr_fn<2, kPow2, kPrec>();
+        case 128: return csr_fn<4, kPow2, kPrec>();
+        case 256: return csr_fn<8, kPow2, kPrec>();
+        default: return nullptr;
+    }
+}
+
+}  // namespace
+
+namespace {
+
+// ELLPACK copy of the CSR couplings: one warp per row, entries [0, row length) from the CSR
+// row in column order, then column -1 / value 0 up to `width`.
+__global__ void ell_fill_kernel(int n, int width, const int32_t* __restrict__ ptr, const int32_t* __restrict__ col,
+                                const double* __restrict__ val64, const float* __restrict__ val32,
+                                int32_t* __restrict__ ell_col, double* __restrict__ ell_val64,
+                                float* __restrict__ ell_val32) {
+    const int lane = threadIdx.x & 31;
+    const int row = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (row >= n) return;
+    const int begin = ptr[row], count = ptr[row + 1] - begin;
+    for (int e = lane; e < width; e += 32) {
+        const size_t at = static_cast<size_t>(row) * width + e;
+        const bool in = e < count;
+        ell_col[at] = in ? col[begin + e] : -1;
+        if (ell_val64) ell_val64[at] = in ? val64[begin + e] : 0.0;
+        if (ell_val32) ell_val32[at] = in ? val32[begin + e] : 0.0f;
+    }
+}
+
+}  // namespace
+
+void launch_ell_fill(int n, int width, const int32_t* ptr, const int32_t* col, const double* val64,
+                     const float* val32, int32_t* ell_col, double* ell_val64, float* ell_val32, cudaStream_t stream) {
+    if (n <= 0) return;
+    const unsigned blocks = static_cast<unsigned>((n + 7) / 8);
+    ell_fill_kernel<<<blocks, 256, 0, stream>>>(n, width, ptr, col, val64, val32, ell_col, ell_val64, ell_val32);
+    check_cuda(cudaGetLastError(), "ell_fill_kernel");
+}
+
+bool launch_sweep_csr(const EngineView& v, const WalkArgs& a, int walkers_per_block, cudaStream_t stream) {
+    if (!v.csr || v.ell_width == 0 || v.p.collect || v.p.nalivaiko) return false;
+    const bool pow2 = v.grid.pow2_width != 0;
+    SweepFn fn = v.precision == WLG_PRECISION_FP32
+                     ? (pow2 ? pick_csr_width<true, WLG_PRECISION_FP32>(v.ell_width)
+                             : pick_csr_width<false, WLG_PRECISION_FP32>(v.ell_width))
+                     : (pow2 ? pick_csr_width<true, WLG_PRECISION_FP64>(v.ell_width)
+                             : pick_csr_width<false, WLG_PRECISION_FP64>(v.ell_width));
+    if (!fn) return false;
+    const size_t per_walker = csr_sweep_layout(v.max_window_bins).total;
+    if (per_walker > 227 * 1024) return false;
+    int wpb = walkers_per_block < 1 ? 1 : (walkers_per_block > 8 ? 8 : walkers_per_block);
+    while (wpb > 1 && per_walker * static_cast<size_t>(wpb) > 227 * 1024) --wpb;
+    const unsigned blocks = static_cast<unsigned>((a.count + wpb - 1) / wpb);
+    fn<<<blocks, 32 * wpb, per_walker * static_cast<size_t>(wpb), stream>>>(v, a);
+    check_cuda(cudaGetLastError(), "sweep_csr_kernel");
+    return true;
+}
+
+}  // namespace wlg

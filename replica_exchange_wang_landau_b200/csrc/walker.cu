@@ -590,6 +590,7 @@ static bool features_of(const EngineView& v) { return v.p.collect || v.p.nalivai
 void launch_walk(const EngineView& v, const WalkArgs& a, int wpb, cudaStream_t stream) {
     const bool features = features_of(v);
     if (!v.csr && launch_sweep_dense(v, a, stream)) return;  // sweep.cu: the TMA row ring
+    if (v.csr && launch_sweep_csr(v, a, wpb, stream)) return;  // sweep_csr.cu: ELLPACK rows, fields in HBM
     const bool smem_fields = a.smem_per_walker >= static_cast<int>(walker_smem_bytes(v, true, features));
     WalkFn fn = pick_walk(v.precision, v.csr != 0, smem_fields, features);
     wpb = std::max(1, std::min(wpb, 8));
