@@ -13,15 +13,17 @@
 //   value 0 pad a row) with lane j holding entries j, j+32, ...: one coalesced load per
 //   chunk and no row-pointer indirection.
 // * The site of the next attempt is draw hq+1 or, when this attempt consumes the acceptance
-//   uniform, draw hq+2 (the lookahead of the dense split sweep).  The warp holds both
-//   candidates' field, spin and couplings row in registers, loaded at least one attempt
-//   ahead.  A candidate's field is loaded after the stores of every earlier flip and is
-//   corrected for the flip of the current attempt when the candidate is a neighbour of the
-//   flipped site (a ballot over the flipped row finds J_ic), and its spin when it is the
-//   flipped site, so it equals the reference's field when the candidate becomes the site:
-//   fma(m, J, f) with m = +-2 rounds the reference's f + m*J once.
-// * At the end of an attempt, after its stores, the warp issues the loads of the next site's
-//   neighbour fields (speculatively: a rejected flip discards them) before the next
+//   uniform, draw hq+2 (the lookahead of the dense split sweep).  The site and both
+//   candidates occupy three slots of a four-slot shared-memory ring: each slot receives by
+//   cp.async (no register is the destination of a load in flight, so advancing the ring is
+//   an index change) the site's couplings row, field and spin word, loaded at least one
+//   attempt ahead and after the stores of every earlier flip.  A candidate is corrected for
+//   the flip of the current attempt when it is a neighbour of the flipped site (a ballot over
+//   the flipped row finds J_ic) and when it is the flipped site, so it equals the reference's
+//   field and spin when it becomes the site: fma(m, J, f) with m = +-2 rounds the reference's
+//   f + m*J once.
+// * At the end of an attempt, after its stores, the warp copies the next site's neighbour
+//   fields into its slot (speculatively: a rejected flip discards them) before the next
 //   acceptance log; the next attempt decides and on acceptance stores
 //   fields[c] = fma(m, J_ic, fields[c]) for every neighbour c.  Each field changes at most
 //   once per flip, so the order of the neighbour updates is immaterial.
@@ -42,18 +44,53 @@ namespace wlg {
 
 namespace {
 
-struct CsrSweepLayout {
-    size_t log_g, hist, hd, active, total;
+// One ring slot: the couplings row (columns, values), the neighbour fields, the site's field
+// and the 32-bit word of the spins array that holds its spin.
+struct CsrSlot {
+    size_t col, val, nf, f, sword, bytes;
 };
-__host__ __device__ inline CsrSweepLayout csr_sweep_layout(int mwb) {
+__host__ __device__ inline CsrSlot csr_slot(int width, int vbytes) {
+    CsrSlot S;
+    size_t at = 0;
+    S.col = at; at += static_cast<size_t>(width) * 4;
+    S.val = at; at += static_cast<size_t>(width) * vbytes;
+    S.nf = at; at += static_cast<size_t>(width) * 8;
+    S.f = at; at += 8;
+    S.sword = at; at += 8;
+    S.bytes = round16(at);
+    return S;
+}
+constexpr int kCsrSlots = 4;
+
+struct CsrSweepLayout {
+    size_t slots, log_g, hist, hd, active, total;
+};
+__host__ __device__ inline CsrSweepLayout csr_sweep_layout(int mwb, int width, int vbytes) {
     CsrSweepLayout L;
     size_t at = 0;
+    L.slots = at; at += kCsrSlots * csr_slot(width, vbytes).bytes;
     L.log_g = at; at += round16(static_cast<size_t>(mwb) * 8);
     L.hist = at; at += round16(static_cast<size_t>(mwb) * 8);
     L.hd = at; at += round16(static_cast<size_t>(mwb) * 4);
     L.active = at; at += round16(static_cast<size_t>(mwb));
     L.total = at;
     return L;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// This thread's copies, all but the newest N groups, have landed.
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 template <int kPrec> struct EllValue { using T = double; };
@@ -65,21 +102,9 @@ __device__ __forceinline__ const typename EllValue<kPrec>::T* ell_values(const E
     else return v.ell_val64;
 }
 
-// One site as the warp holds it: field, spin and this lane's entries of its couplings row.
-template <int kK, class VT>
-struct SiteRegs {
-    int site;  // -1: the draw is rejected by bounded()
-    double f;
-    int s;
-    int col[kK];
-    VT val[kK];
-    double nf[kK];  // the neighbour fields (loaded when the site is next)
-};
-
 template <int kK, bool kPow2, int kPrec>
 __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArgs a) {
     using VT = typename EllValue<kPrec>::T;
-    using Site = SiteRegs<kK, VT>;
     constexpr int kWidth = 32 * kK;
     extern __shared__ __align__(16) unsigned char smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -89,8 +114,11 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
     Control* ctl = v.ctl;
     if (a.epoch_mode && *reinterpret_cast<volatile int32_t*>(&ctl->done)) return;
 
-    const CsrSweepLayout L = csr_sweep_layout(v.max_window_bins);
+    const CsrSweepLayout L = csr_sweep_layout(v.max_window_bins, kWidth, sizeof(VT));
+    const CsrSlot S = csr_slot(kWidth, sizeof(VT));
     unsigned char* base = smem + static_cast<size_t>(warp) * L.total;
+    unsigned char* ring = base + L.slots;
+    const uint32_t ring_addr = static_cast<uint32_t>(__cvta_generic_to_shared(ring));
     double* lg_s = reinterpret_cast<double*>(base + L.log_g);
     uint64_t* h_s = reinterpret_cast<uint64_t*>(base + L.hist);
     uint32_t* hd = reinterpret_cast<uint32_t*>(base + L.hd);
@@ -128,32 +156,58 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
     __syncwarp();
 
     auto site_of = [&](uint64_t d) -> int { return d < fm.threshold ? -1 : static_cast<int>(fast_mod(fm, d)); };
-    // issue the loads of one site's field, spin and row (the field and spin as stored now)
-    auto fetch = [&](int site, Site& c) {
-        c.site = site;
+    auto slot_ptr = [&](int k) { return ring + static_cast<size_t>(k & (kCsrSlots - 1)) * S.bytes; };
+    auto slot_addr = [&](int k) { return ring_addr + static_cast<uint32_t>((k & (kCsrSlots - 1)) * S.bytes); };
+    // copy one site's row, field and spin word into ring slot k (one commit group)
+    auto fetch = [&](int k, int site) {
         const int s = site < 0 ? 0 : site;
-        c.f = fg[s];
-        c.s = sg[s];
-        const size_t r = static_cast<size_t>(s) * kWidth + static_cast<size_t>(lane);
+        const uint32_t dst = slot_addr(k);
+        const unsigned char* crow = reinterpret_cast<const unsigned char*>(ecol + static_cast<size_t>(s) * kWidth);
+        const unsigned char* vrow = reinterpret_cast<const unsigned char*>(evals + static_cast<size_t>(s) * kWidth);
 #pragma unroll
-        for (int k = 0; k < kK; ++k) {
-            c.col[k] = __ldg(ecol + r + 32 * k);
-            c.val[k] = __ldg(evals + r + 32 * k);
-        }
+        for (int c = lane; c < kWidth * 4 / 16; c += 32) cp_async16(dst + static_cast<uint32_t>(S.col + 16 * c), crow + 16 * c);
+#pragma unroll
+        for (int c = lane; c < kWidth * static_cast<int>(sizeof(VT)) / 16; c += 32)
+            cp_async16(dst + static_cast<uint32_t>(S.val + 16 * c), vrow + 16 * c);
+        if (lane == 0) cp_async8(dst + static_cast<uint32_t>(S.f), fg + s);
+        if (lane == 1) cp_async4(dst + static_cast<uint32_t>(S.sword), sg + (s & ~3));
+        cp_commit();
     };
-    // a candidate after the accepted flip of `flipped` with factor m
-    auto correct = [&](Site& c, const Site& flipped, double m) {
+    // copy the neighbour fields of the site in slot k (lane j: entries j, j+32, ...; one group)
+    auto load_neighbours = [&](int k) {
+        const unsigned char* p = slot_ptr(k);
+        const uint32_t dst = slot_addr(k);
+#pragma unroll
+        for (int e = 0; e < kK; ++e) {
+            const int c = reinterpret_cast<const int32_t*>(p + S.col)[lane + 32 * e];
+            if (c >= 0) cp_async8(dst + static_cast<uint32_t>(S.nf + 8 * (lane + 32 * e)), fg + c);
+        }
+        cp_commit();
+    };
+    auto slot_field = [&](int k) -> double& { return *reinterpret_cast<double*>(slot_ptr(k) + S.f); };
+    auto slot_spin = [&](int k, int site) -> int {
+        const uint32_t word = *reinterpret_cast<const uint32_t*>(slot_ptr(k) + S.sword);
+        return static_cast<int8_t>(static_cast<uint8_t>(word >> (8 * (site & 3))));
+    };
+    // the candidate `site` in slot k after the accepted flip of `flipped` (slot kf), factor m;
+    // every copy has landed
+    auto correct = [&](int k, int site, int kf, int flipped, double m) {
+        const unsigned char* pf = slot_ptr(kf);
         bool hit = false;
         double jv = 0.0;
 #pragma unroll
-        for (int k = 0; k < kK; ++k)
-            if (c.site >= 0 && flipped.col[k] == c.site) {
+        for (int e = 0; e < kK; ++e)
+            if (site >= 0 && reinterpret_cast<const int32_t*>(pf + S.col)[lane + 32 * e] == site) {
                 hit = true;
-                jv = static_cast<double>(flipped.val[k]);
+                jv = static_cast<double>(reinterpret_cast<const VT*>(pf + S.val)[lane + 32 * e]);
             }
         const unsigned mask = __ballot_sync(kFull, hit);
-        if (mask) c.f = fma(m, __shfl_sync(kFull, jv, __ffs(mask) - 1), c.f);
-        if (c.site == flipped.site) c.s = -c.s;
+        if (mask) {
+            jv = __shfl_sync(kFull, jv, __ffs(mask) - 1);
+            if (lane == 0) slot_field(k) = fma(m, jv, slot_field(k));
+        }
+        if (site == flipped && lane == 1)  // the spin byte: +1 (0x01) <-> -1 (0xff)
+            *reinterpret_cast<uint32_t*>(slot_ptr(k) + S.sword) ^= 0xfeu << (8 * (site & 3));
     };
 
     double E = st.energy;
@@ -175,22 +229,19 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
         active_before = warp_sum_u64(active_before);
     }
 
-    // Three register sets hold the site of the next attempt (draw hq) and the candidates
-    // (draws hq+1, hq+2); their roles rotate by one or two places per attempt.  The rotation
-    // is a switch over the three role assignments, not register moves: a move of a set whose
-    // loads are still in flight would wait for them.
+    // Slots o, o+1, o+2 (mod 4) hold the site of the next attempt (draw hq) and the candidates
+    // (draws hq+1, hq+2); site indices i0, i1, i2.
     Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};
-    Site A, B, C;
-    fetch(site_of(rng.next()), A);
+    int o = 0;
+    int i0 = site_of(rng.next());
     uint64_t d1 = rng.next(), d2 = rng.next();
-    fetch(site_of(d1), B);
-    fetch(site_of(d2), C);
-    // the neighbour fields of a site, loaded before its attempt (after every earlier store)
-    auto load_neighbours = [&](Site& c) {
-#pragma unroll
-        for (int k = 0; k < kK; ++k) c.nf[k] = c.col[k] >= 0 ? fg[c.col[k]] : 0.0;
-    };
-    load_neighbours(A);
+    int i1 = site_of(d1), i2 = site_of(d2);
+    fetch(0, i0);
+    fetch(1, i1);
+    fetch(2, i2);
+    cp_wait<0>();
+    __syncwarp();
+    load_neighbours(0);
     double lnu = log(fmax(to_uniform(d1), 0x1.0p-53));
 
     // The attempts of one batch; kIT selects the 1/t stage (per-attempt factor and active
@@ -200,20 +251,25 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
         const bool frozen = stage == kFrozen;
         double factor_next = factor;
         if (kIT && active_count != 0) factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + 1);
-        uint32_t t = 0;
-        // One attempt with the roles (site, c1, c2); returns the rotation of the roles.
-        auto attempt = [&](Site& site, Site& c1, Site& c2) -> int {
-            if (site.site < 0) {  // rare: bounded() rejects draw hq; the next draw is the site
+        for (uint32_t t = 0; t < batch;) {
+            if (i0 < 0) {  // rare: bounded() rejects draw hq; the next draw is the site
                 d1 = d2;
                 d2 = rng.next();
-                fetch(site_of(d2), site);  // becomes c2
-                load_neighbours(c1);
+                i0 = i1;
+                i1 = i2;
+                i2 = site_of(d2);
+                fetch(o + 3, i2);
+                o = (o + 1) & (kCsrSlots - 1);
+                cp_wait<2>();  // the new site's row (an older group) has landed
+                __syncwarp();
+                load_neighbours(o);
                 lnu = log(fmax(to_uniform(d1), 0x1.0p-53));
-                return 1;
+                continue;
             }
             // the decision (attempt_flip, src/wang_landau.cpp:244-262)
-            const double m = site.s > 0 ? -2.0 : 2.0;  // -2 * spin
-            const double Ep = fma(m, site.f, E);
+            const int si = slot_spin(o, i0);
+            const double m = si > 0 ? -2.0 : 2.0;  // -2 * spin
+            const double Ep = fma(m, slot_field(o), E);
             const bool in_range = Ep >= g.minimum && Ep <= g.maximum;
             const double qv = kPow2 ? fma(Ep, g.inv_width, neg_min_scaled) : (Ep - g.minimum) / g.width;
             int nb = in_range ? __double2int_rd(qv) : -1;
@@ -228,12 +284,20 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
             const bool accepted = in_window && (det || forced || lnu < log_ratio);
 
             if (accepted) {  // add_flip_delta, and the candidates brought up to date
+                cp_wait<0>();
+                __syncwarp();
+                const unsigned char* ps = slot_ptr(o);
 #pragma unroll
-                for (int k = 0; k < kK; ++k)
-                    if (site.col[k] >= 0) fg[site.col[k]] = fma(m, static_cast<double>(site.val[k]), site.nf[k]);
-                if (lane == 0) sg[site.site] = static_cast<int8_t>(-site.s);
-                correct(c2, site, m);
-                if (!need_u) correct(c1, site, m);  // draw hq+1 becomes the next site
+                for (int e = 0; e < kK; ++e) {
+                    const int j = lane + 32 * e;
+                    const int c = reinterpret_cast<const int32_t*>(ps + S.col)[j];
+                    if (c >= 0)
+                        fg[c] = fma(m, static_cast<double>(reinterpret_cast<const VT*>(ps + S.val)[j]),
+                                    reinterpret_cast<const double*>(ps + S.nf)[j]);
+                }
+                if (lane == 0) sg[i0] = static_cast<int8_t>(-si);
+                correct(o + 2, i2, o, i0, m);
+                if (!need_u) correct(o + 1, i1, o, i0, m);  // draw hq+1 becomes the next site
             }
             E = accepted ? Ep : E;
             since = accepted ? 0 : since + 1;
@@ -267,39 +331,37 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
                 lg_cur = frozen ? lg_base : lg_base + factor;
             }
 
-            __syncwarp();  // this attempt's stores are visible to every lane before later loads
-            int rotation;
+            __syncwarp();  // this attempt's stores and reads of the slots precede later copies
             if (need_u) {  // draw hq+1 was the uniform: the site is draw hq+2
                 d1 = rng.next();
                 d2 = rng.next();
-                load_neighbours(c2);
-                fetch(site_of(d1), site);  // becomes c1
-                fetch(site_of(d2), c1);    // becomes c2
-                rotation = 2;
+                i0 = i2;
+                i1 = site_of(d1);
+                i2 = site_of(d2);
+                fetch(o + 3, i1);
+                fetch(o + 4, i2);  // the slot of the site just done
+                o = (o + 2) & (kCsrSlots - 1);
+                cp_wait<3>();  // the new site's row (older than the last three groups) has landed
             } else {
                 d1 = d2;
                 d2 = rng.next();
-                load_neighbours(c1);
-                fetch(site_of(d2), site);  // becomes c2
-                rotation = 1;
+                i0 = i1;
+                i1 = i2;
+                i2 = site_of(d2);
+                fetch(o + 3, i2);
+                o = (o + 1) & (kCsrSlots - 1);
+                cp_wait<2>();
             }
+            __syncwarp();
+            load_neighbours(o);  // issued before the log below, so that its latency overlaps it
             lnu = log(fmax(to_uniform(d1), 0x1.0p-53));
-            return rotation;
-        };
-        int roles = 0;  // 0: (A, B, C), 1: (B, C, A), 2: (C, A, B)
-        while (t < batch) {
-            int r;
-            if (roles == 0) r = attempt(A, B, C);
-            else if (roles == 1) r = attempt(B, C, A);
-            else r = attempt(C, A, B);
-            roles += r;
-            roles = roles >= 3 ? roles - 3 : roles;
         }
     };
     if (stage == kInverseTime)
         run(std::true_type{});
     else
         run(std::false_type{});
+    cp_wait<0>();  // no copy is in flight when the walker leaves
 
     // the generator is three draws past the last consumed one (the next site, hq+1, hq+2)
     rng_step_back(rng);
@@ -420,7 +482,8 @@ bool launch_sweep_csr(const EngineView& v, const WalkArgs& a, int walkers_per_bl
                      : (pow2 ? pick_csr_width<true, WLG_PRECISION_FP64>(v.ell_width)
                              : pick_csr_width<false, WLG_PRECISION_FP64>(v.ell_width));
     if (!fn) return false;
-    const size_t per_walker = csr_sweep_layout(v.max_window_bins).total;
+    const int vbytes = v.precision == WLG_PRECISION_FP32 ? 4 : 8;
+    const size_t per_walker = csr_sweep_layout(v.max_window_bins, v.ell_width, vbytes).total;
     if (per_walker > 227 * 1024) return false;
     int wpb = walkers_per_block < 1 ? 1 : (walkers_per_block > 8 ? 8 : walkers_per_block);
     while (wpb > 1 && per_walker * static_cast<size_t>(wpb) > 227 * 1024) --wpb;
