@@ -115,6 +115,7 @@ class Oracle(_Checker):
             "orc_couplings_size": (_u64, [_vp]),
             "orc_couplings_nnz": (_u64, [_vp]),
             "orc_couplings_set_update_fp32": (None, [_vp, C.c_int]),
+            "orc_couplings_csr": (None, [_vp, P(_u64), P(_u64), P(_dbl)]),
             "orc_couplings_dense": (None, [_vp, P(_dbl)]),
             "orc_local_fields": (None, [_vp, P(C.c_int8), P(_dbl)]),
             "orc_total_energy": (_dbl, [_vp, P(C.c_int8)]),
@@ -170,6 +171,20 @@ class Oracle(_Checker):
         nnz = int(self.lib.orc_couplings_nnz(h))
         self.lib.orc_couplings_destroy(h)
         return nnz
+
+    def csr(self, system: System):
+        """(offsets, columns, values) of the restated CsrCouplings."""
+        h = self._couplings(system)
+        try:
+            n = system.size()
+            nnz = int(self.lib.orc_couplings_nnz(h))
+            ptr = np.zeros(n + 1, np.uint64)
+            cols = np.zeros(max(1, nnz), np.uint64)
+            vals = np.zeros(max(1, nnz), np.float64)
+            self.lib.orc_couplings_csr(h, _u64ptr(ptr), _u64ptr(cols), _dptr(vals))
+            return ptr, cols[:nnz], vals[:nnz]
+        finally:
+            self.lib.orc_couplings_destroy(h)
 
     def local_fields(self, system: System, spins: np.ndarray):
         h = self._couplings(system)

@@ -268,6 +268,14 @@ static void add_flip_delta(const orc_couplings* c, uint64_t flipped, int8_t old_
 
 void orc_couplings_set_update_fp32(orc_couplings* c, int on) { c->update_fp32 = on != 0; }
 
+void orc_couplings_csr(const orc_couplings* c, uint64_t* offsets, uint64_t* columns, double* values) {
+    if (!c->csr) return;
+    const uint64_t nnz = c->offsets[c->n];
+    memcpy(offsets, c->offsets, (c->n + 1) * sizeof(uint64_t));
+    memcpy(columns, c->columns, nnz * sizeof(uint64_t));
+    memcpy(values, c->values, nnz * sizeof(double));
+}
+
 /* ---- energy grid and windows (src/wang_landau.cpp:13-61) ---------------------- */
 
 /* EnergyGrid::validate (wang_landau.cpp:13-20) */

@@ -32,6 +32,8 @@ uint64_t orc_couplings_nnz(const orc_couplings* c);
  * FP64.  Set it after a walker's construction to follow an FP32 engine walker, whose
  * initialisation uses the FP64 couplings. */
 void orc_couplings_set_update_fp32(orc_couplings* c, int on);
+/* The CSR arrays of a cutoff system: offsets[n+1], columns[nnz], values[nnz]. */
+void orc_couplings_csr(const orc_couplings* c, uint64_t* offsets, uint64_t* columns, double* values);
 void orc_couplings_dense(const orc_couplings* c, double* out);
 void orc_local_fields(const orc_couplings* c, const int8_t* spins, double* fields);
 double orc_total_energy(const orc_couplings* c, const int8_t* spins);

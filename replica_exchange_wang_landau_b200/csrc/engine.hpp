@@ -86,6 +86,10 @@ struct DeviceSystem {
     DeviceBuffer csr_ptr, csr_col, csr_val64, csr_val32;
     DeviceBuffer ell_col, ell_val64, ell_val32;  // ELLPACK rows for the CSR sweep
     int32_t ell_width = 0;                       // entries per row (0: not built)
+    // cell grid of the CSR build: sites sorted by cell, cells at least the cutoff wide
+    DeviceBuffer cell_start, cell_sites, site_cell;
+    int32_t cells[3] = {1, 1, 1};
+    int32_t cell_wrap[3] = {0, 0, 0};
 };
 
 // Host-side validation and helpers (host.cpp).
@@ -94,6 +98,7 @@ void validate_grid(double emin, double emax, double width);
 uint64_t grid_bins(double emin, double emax, double width);
 std::vector<uint64_t> partition_windows(uint64_t bins, uint64_t count, double overlap);
 void upload_system(const wlg_system& s, DeviceSystem& d, cudaStream_t stream);
+void upload_cell_grid(const wlg_system& s, DeviceSystem& d, cudaStream_t stream);
 void save_checkpoint_file(const std::string& path, const wlg_snapshot& s, uint64_t n, uint64_t bins);
 bool load_checkpoint_file(const std::string& path, std::vector<int8_t>& spins, std::vector<double>& fields,
                           std::vector<double>& log_g, std::vector<uint64_t>& hist, std::vector<uint8_t>& active,

@@ -5,6 +5,7 @@
 #include <filesystem>
 #include <fstream>
 #include <limits>
+#include <vector>
 
 #include "engine.hpp"
 
@@ -88,6 +89,89 @@ void upload_system(const wlg_system& s, DeviceSystem& d, cudaStream_t stream) {
                "copy positions");
     check_cuda(cudaMemcpyAsync(d.axes.ptr, s.axes, s.n * 3 * sizeof(double), cudaMemcpyHostToDevice, stream),
                "copy axes");
+    if (d.csr) upload_cell_grid(s, d, stream);
+}
+
+// The cell grid of the CSR build.  Along a periodic axis (box length L > 0) the cells divide
+// [0, L) into nc = floor(L / w) equal cells, w = cutoff * (1 + 1e-6), and a position is
+// wrapped into [0, L) first; along an open axis they are w wide from the smallest
+// coordinate.  Every cell is then wider than the cutoff, so two sites whose minimum-image
+// distance is within the cutoff lie in the same or adjacent cells (adjacency wrapping
+// around periodic axes); the slack of 1e-6 covers rounding in the cell assignment.  A
+// periodic axis with fewer than three cells becomes a single cell, since its neighbours on
+// both sides would coincide.  The grid is coarsened (never below the cutoff width) when it
+// would have more than 8n + 64 cells.  Sites are listed per cell in increasing index.
+void upload_cell_grid(const wlg_system& s, DeviceSystem& d, cudaStream_t stream) {
+    const uint64_t n = s.n;
+    const double w = s.cutoff * (1.0 + 1e-6);
+    int64_t nc[3];
+    double lo[3], extent[3], width[3];
+    bool wrap[3];
+    for (int k = 0; k < 3; ++k) {
+        wrap[k] = s.periodic != 0 && s.box[k] > 0.0;
+        double mn = std::numeric_limits<double>::infinity(), mx = -mn;
+        for (uint64_t i = 0; i < n; ++i) {
+            mn = std::min(mn, s.positions[3 * i + k]);
+            mx = std::max(mx, s.positions[3 * i + k]);
+        }
+        lo[k] = mn;
+        extent[k] = mx - mn;
+        if (wrap[k]) {
+            const double cells = std::min(std::floor(s.box[k] / w), 4096.0);
+            nc[k] = cells >= 3.0 ? static_cast<int64_t>(cells) : 1;
+            width[k] = s.box[k] / static_cast<double>(nc[k]);
+        } else {
+            width[k] = extent[k] / w > 4095.0 ? extent[k] / 4095.0 : w;
+            nc[k] = static_cast<int64_t>(std::floor(extent[k] / width[k])) + 1;
+        }
+    }
+    const auto total = [&]() { return nc[0] * nc[1] * nc[2]; };
+    while (total() > static_cast<int64_t>(8 * n + 64)) {
+        int k = 0;
+        for (int q = 1; q < 3; ++q)
+            if (nc[q] > nc[k]) k = q;
+        if (wrap[k]) {
+            nc[k] = nc[k] / 2 >= 3 ? nc[k] / 2 : 1;
+            width[k] = s.box[k] / static_cast<double>(nc[k]);
+        } else {
+            width[k] *= 2.0;
+            nc[k] = static_cast<int64_t>(std::floor(extent[k] / width[k])) + 1;
+        }
+    }
+    std::vector<int32_t> cell_of(n), count(static_cast<size_t>(total()) + 1, 0);
+    for (uint64_t i = 0; i < n; ++i) {
+        int64_t c[3];
+        for (int k = 0; k < 3; ++k) {
+            const double x = s.positions[3 * i + k];
+            double u;
+            if (wrap[k]) {
+                u = x / s.box[k];
+                u = (u - std::floor(u)) * static_cast<double>(nc[k]);
+            } else {
+                u = (x - lo[k]) / width[k];
+            }
+            c[k] = std::min<int64_t>(nc[k] - 1, std::max<int64_t>(0, static_cast<int64_t>(u)));
+        }
+        cell_of[i] = static_cast<int32_t>(c[0] + nc[0] * (c[1] + nc[1] * c[2]));
+        ++count[static_cast<size_t>(cell_of[i]) + 1];
+    }
+    for (size_t c = 1; c < count.size(); ++c) count[c] += count[c - 1];
+    std::vector<int32_t> sites(n), fill(count.begin(), count.end() - 1);
+    for (uint64_t i = 0; i < n; ++i) sites[static_cast<size_t>(fill[static_cast<size_t>(cell_of[i])]++)] = static_cast<int32_t>(i);
+    for (int k = 0; k < 3; ++k) {
+        d.cells[k] = static_cast<int32_t>(nc[k]);
+        d.cell_wrap[k] = wrap[k] ? 1 : 0;
+    }
+    d.cell_start.allocate(count.size() * sizeof(int32_t));
+    d.cell_sites.allocate(n * sizeof(int32_t));
+    d.site_cell.allocate(n * sizeof(int32_t));
+    check_cuda(cudaMemcpyAsync(d.cell_start.ptr, count.data(), d.cell_start.bytes, cudaMemcpyHostToDevice, stream),
+               "copy cells");
+    check_cuda(cudaMemcpyAsync(d.cell_sites.ptr, sites.data(), d.cell_sites.bytes, cudaMemcpyHostToDevice, stream),
+               "copy cells");
+    check_cuda(cudaMemcpyAsync(d.site_cell.ptr, cell_of.data(), d.site_cell.bytes, cudaMemcpyHostToDevice, stream),
+               "copy cells");
+    check_cuda(cudaStreamSynchronize(stream), "sync");  // the host vectors go out of scope
 }
 
 // ---- checkpoint (src/io.cpp:539-572) ---------------------------------------------------

@@ -4,9 +4,13 @@
 //    pairs (i < j) per CTA; each pair is evaluated once, in the reference's orientation
 //    (displacement r_j - r_i, axes e_i then e_j), and written to both triangles through a
 //    shared-memory transpose so both stores are coalesced.
-//  * csr_count_kernel / csr_fill_kernel: CsrCouplings (src/physics.cpp:197-223).  One warp
-//    per row; columns are visited in increasing order and compacted with a ballot, which
-//    yields the reference's (row, column) sort order without sorting.
+//  * csr_count_kernel / csr_fill_kernel: CsrCouplings (src/physics.cpp:197-223) from a cell
+//    grid (cells wider than the cutoff, built on the host at upload): one warp per row visits
+//    the sites of its cell and the adjacent ones, evaluates each pair once in the reference's
+//    orientation and keeps those within the cutoff, O(N z) instead of the reference's O(N^2)
+//    scan.  The row is then sorted by column in shared memory (a bitonic network), which
+//    gives the reference's (row, column) order; rows longer than the sort buffer take the
+//    scan over all columns in increasing order (csr_scan_fill_kernel).
 //  * fields_kernel / energy_kernel: local_fields and total_energy (src/physics.cpp:
 //    238-259) with the reference's sequential summation order.
 //
@@ -24,6 +28,12 @@ struct SystemView {
     double scale;
     double cutoff;
     int32_t n;
+    // the cell grid (CSR only)
+    const int32_t* cell_start;  // cells + 1
+    const int32_t* cell_sites;  // n, grouped by cell
+    const int32_t* site_cell;   // n
+    int32_t nc[3];
+    int32_t wrap[3];
 };
 
 // minimum_image (src/physics.cpp:151-160)
@@ -77,31 +87,151 @@ __global__ void dense_build_kernel(SystemView s, int ld, double* __restrict__ J,
     }
 }
 
-// One warp per row: count the columns c != row with norm(d) <= cutoff.
+// Calls f(cell) for the cell of `site` and the cells adjacent to it (at most 27, each once).
+template <class F>
+__device__ __forceinline__ void for_adjacent_cells(const SystemView& s, int site, F&& f) {
+    const int cell = s.site_cell[site];
+    const int c0 = cell % s.nc[0], c1 = (cell / s.nc[0]) % s.nc[1], c2 = cell / (s.nc[0] * s.nc[1]);
+    const int r0 = s.nc[0] > 1 ? 1 : 0, r1 = s.nc[1] > 1 ? 1 : 0, r2 = s.nc[2] > 1 ? 1 : 0;
+    for (int d2 = -r2; d2 <= r2; ++d2) {
+        int z = c2 + d2;
+        if (s.wrap[2]) z = z < 0 ? z + s.nc[2] : (z >= s.nc[2] ? z - s.nc[2] : z);
+        else if (z < 0 || z >= s.nc[2]) continue;
+        for (int d1 = -r1; d1 <= r1; ++d1) {
+            int y = c1 + d1;
+            if (s.wrap[1]) y = y < 0 ? y + s.nc[1] : (y >= s.nc[1] ? y - s.nc[1] : y);
+            else if (y < 0 || y >= s.nc[1]) continue;
+            for (int d0 = -r0; d0 <= r0; ++d0) {
+                int x = c0 + d0;
+                if (s.wrap[0]) x = x < 0 ? x + s.nc[0] : (x >= s.nc[0] ? x - s.nc[0] : x);
+                else if (x < 0 || x >= s.nc[0]) continue;
+                f(x + s.nc[0] * (y + s.nc[1] * z));
+            }
+        }
+    }
+}
+
+// One warp per row: count the columns c != row with norm(d) <= cutoff among the sites of the
+// adjacent cells.
 __global__ void csr_count_kernel(SystemView s, int32_t* __restrict__ counts, int* __restrict__ err) {
     const int lane = threadIdx.x & 31;
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int row = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (row >= s.n) return;
     int total = 0;
-    for (int c0 = 0; c0 < s.n; c0 += 32) {
-        const int c = c0 + lane;
-        bool in = false;
-        if (c < s.n && c != row) {
-            double v, dist;
-            const bool ok = pair_value(s, min(row, c), max(row, c), v, dist);
-            in = dist <= s.cutoff;
-            if (in && !ok) atomicExch(err, 1);
+    for_adjacent_cells(s, row, [&](int cell) {
+        const int end = s.cell_start[cell + 1];
+        for (int q0 = s.cell_start[cell]; q0 < end; q0 += 32) {
+            const int q = q0 + lane;
+            bool in = false;
+            if (q < end) {
+                const int c = s.cell_sites[q];
+                if (c != row) {
+                    double v, dist;
+                    const bool ok = pair_value(s, min(row, c), max(row, c), v, dist);
+                    in = dist <= s.cutoff;
+                    if (in && !ok) atomicExch(err, 1);
+                }
+            }
+            total += __popc(__ballot_sync(0xffffffffu, in));
         }
-        total += __popc(__ballot_sync(0xffffffffu, in));
-    }
+    });
     if (lane == 0) counts[row] = total;
 }
 
-__global__ void csr_fill_kernel(SystemView s, const int32_t* __restrict__ ptr, int32_t* __restrict__ col,
-                                double* __restrict__ val64, float* __restrict__ val32) {
-    const int lane = threadIdx.x & 31;
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+constexpr int kSortCapacity = 1024;  // entries of the per-warp row sort buffer
+constexpr int kFillWarps = 4;
+
+// One warp per row: the row's (column, value) pairs from the adjacent cells into shared
+// memory, sorted by column with a bitonic network, then stored at ptr[row].  Rows with more
+// than kSortCapacity entries are listed in `overflow` for csr_scan_fill_kernel.
+__global__ void __launch_bounds__(32 * kFillWarps) csr_fill_kernel(SystemView s, const int32_t* __restrict__ ptr,
+                                                                   int32_t* __restrict__ col,
+                                                                   double* __restrict__ val64,
+                                                                   float* __restrict__ val32,
+                                                                   int32_t* __restrict__ overflow,
+                                                                   int* __restrict__ overflow_count) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int row = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (row >= s.n) return;
+    const int count = ptr[row + 1] - ptr[row];
+    if (count > kSortCapacity) {
+        if (lane == 0) overflow[atomicAdd(overflow_count, 1)] = row;
+        return;
+    }
+    double* vs = reinterpret_cast<double*>(smem) + static_cast<size_t>(warp) * kSortCapacity;
+    int32_t* cs = reinterpret_cast<int32_t*>(smem + static_cast<size_t>(kFillWarps) * kSortCapacity * 8) +
+                  static_cast<size_t>(warp) * kSortCapacity;
+    int at = 0;
+    for_adjacent_cells(s, row, [&](int cell) {
+        const int end = s.cell_start[cell + 1];
+        for (int q0 = s.cell_start[cell]; q0 < end; q0 += 32) {
+            const int q = q0 + lane;
+            bool in = false;
+            int c = 0;
+            double v = 0.0;
+            if (q < end) {
+                c = s.cell_sites[q];
+                if (c != row) {
+                    double dist;
+                    pair_value(s, min(row, c), max(row, c), v, dist);
+                    in = dist <= s.cutoff;
+                }
+            }
+            const unsigned mask = __ballot_sync(0xffffffffu, in);
+            if (in) {
+                const int e = at + __popc(mask & ((1u << lane) - 1u));
+                if (e < kSortCapacity) {
+                    cs[e] = c;
+                    vs[e] = v;
+                }
+            }
+            at += __popc(mask);
+        }
+    });
+    int padded = 1;
+    while (padded < count) padded <<= 1;
+    for (int e = count + lane; e < padded; e += 32) {
+        cs[e] = 0x7fffffff;
+        vs[e] = 0.0;
+    }
+    __syncwarp();
+    for (int k = 2; k <= padded; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < padded; i += 32) {
+                const int partner = i ^ j;
+                if (partner > i) {
+                    const bool ascending = (i & k) == 0;
+                    const int a = cs[i], b = cs[partner];
+                    if ((a > b) == ascending) {
+                        cs[i] = b;
+                        cs[partner] = a;
+                        const double t = vs[i];
+                        vs[i] = vs[partner];
+                        vs[partner] = t;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    const int base = ptr[row];
+    for (int e = lane; e < count; e += 32) {
+        col[base + e] = cs[e];
+        val64[base + e] = vs[e];
+        if (val32) val32[base + e] = static_cast<float>(vs[e]);
+    }
+}
+
+// One warp per listed row: all columns in increasing order, compacted with a ballot (the
+// reference's order without sorting; O(N) per row).
+__global__ void csr_scan_fill_kernel(SystemView s, const int32_t* __restrict__ rows, int count,
+                                     const int32_t* __restrict__ ptr, int32_t* __restrict__ col,
+                                     double* __restrict__ val64, float* __restrict__ val32) {
+    const int lane = threadIdx.x & 31;
+    const int k = static_cast<int>((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (k >= count) return;
+    const int row = rows[k];
     int base = ptr[row];
     for (int c0 = 0; c0 < s.n; c0 += 32) {
         const int c = c0 + lane;
@@ -181,7 +311,7 @@ __global__ void energy_kernel(int n, const int8_t* __restrict__ spins, int64_t s
 // ---- host launchers ------------------------------------------------------------------
 
 static SystemView make_view(const DeviceSystem& d) {
-    SystemView s;
+    SystemView s{};
     s.pos = d.pos.get<double>();
     s.axes = d.axes.get<double>();
     for (int k = 0; k < 3; ++k) s.box[k] = d.box[k];
@@ -189,12 +319,19 @@ static SystemView make_view(const DeviceSystem& d) {
     s.scale = d.scale;
     s.cutoff = d.cutoff;
     s.n = static_cast<int32_t>(d.n);
+    s.cell_start = d.cell_start.get<int32_t>();
+    s.cell_sites = d.cell_sites.get<int32_t>();
+    s.site_cell = d.site_cell.get<int32_t>();
+    for (int k = 0; k < 3; ++k) {
+        s.nc[k] = d.cells[k];
+        s.wrap[k] = d.cell_wrap[k];
+    }
     return s;
 }
 
 void launch_dense_build(const double* pos, const double* axes, const double* box, int periodic, double scale, int n,
                         int ld, double* J, int* err, cudaStream_t stream) {
-    SystemView s;
+    SystemView s{};
     s.pos = pos;
     s.axes = axes;
     for (int k = 0; k < 3; ++k) s.box[k] = box[k];
@@ -255,11 +392,24 @@ void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream) {
         d.csr_col.allocate(nnz * sizeof(int32_t));
         d.csr_val64.allocate(nnz * sizeof(double));
         if (precision == WLG_PRECISION_FP32) d.csr_val32.allocate(nnz * sizeof(float));
-        csr_fill_kernel<<<blocks, 32 * warps_per_block, 0, stream>>>(s, d.csr_ptr.get<int32_t>(),
-                                                                     d.csr_col.get<int32_t>(),
-                                                                     d.csr_val64.get<double>(),
-                                                                     d.csr_val32.get<float>());
+        DeviceBuffer overflow(static_cast<size_t>(n) * sizeof(int32_t) + sizeof(int));
+        int* overflow_count = reinterpret_cast<int*>(overflow.get<unsigned char>() + static_cast<size_t>(n) * 4);
+        check_cuda(cudaMemsetAsync(overflow_count, 0, sizeof(int), stream), "memset");
+        const size_t fill_smem = static_cast<size_t>(kFillWarps) * kSortCapacity * (8 + 4);
+        csr_fill_kernel<<<static_cast<unsigned>((n + kFillWarps - 1) / kFillWarps), 32 * kFillWarps, fill_smem, stream>>>(
+            s, d.csr_ptr.get<int32_t>(), d.csr_col.get<int32_t>(), d.csr_val64.get<double>(), d.csr_val32.get<float>(),
+            overflow.get<int32_t>(), overflow_count);
         check_cuda(cudaGetLastError(), "csr_fill_kernel");
+        int long_rows = 0;
+        check_cuda(cudaMemcpyAsync(&long_rows, overflow_count, sizeof(int), cudaMemcpyDeviceToHost, stream), "copy");
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        if (long_rows > 0) {
+            csr_scan_fill_kernel<<<static_cast<unsigned>((long_rows + warps_per_block - 1) / warps_per_block),
+                                   32 * warps_per_block, 0, stream>>>(s, overflow.get<int32_t>(), long_rows,
+                                                                      d.csr_ptr.get<int32_t>(), d.csr_col.get<int32_t>(),
+                                                                      d.csr_val64.get<double>(), d.csr_val32.get<float>());
+            check_cuda(cudaGetLastError(), "csr_scan_fill_kernel");
+        }
         // the ELLPACK copy read by the CSR sweep (rows of at most 256 couplings)
         int32_t zmax = 0;
         for (int32_t c : host_counts) zmax = std::max(zmax, c);

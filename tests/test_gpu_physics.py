@@ -67,6 +67,34 @@ def test_csr_structure(oracle):
         assert same_double(vals[ptr[i]:ptr[i + 1]], dense[i, row.astype(np.int64)])
 
 
+def _cell_systems():
+    """Cutoff systems whose cell grid has several cells per axis, or overflows the row sort."""
+    from replica_exchange_wang_landau_b200.geometry import random_sequential, simple_cubic_random
+    out = {}
+    out["periodic12_r2.5"] = System(simple_cubic_random(12, 12, 12, seed=31), 1.0, 2.5)  # 4 cells per axis
+    out["periodic12_r3.0"] = System(simple_cubic_random(12, 12, 12, seed=32), 1.0, 3.0)  # 3 cells, pairs at exactly r
+    shifted = simple_cubic_random(10, 9, 8, seed=33)
+    shifted.positions = shifted.positions + np.array([-7.3, 23.9, -100.25])  # wrapped into the box by the grid
+    out["shifted_r2.0"] = System(shifted, 1.0, 2.0)
+    out["slab12x12x10_r2.0"] = System(simple_cubic_random(12, 12, 10, seed=34, box=(12.0, 12.0, 0.0)), 1.0, 2.0)
+    out["open10_r2.2"] = System(simple_cubic_random(10, 10, 10, seed=35, periodic=False), 1.0, 2.2)
+    out["dilute1000_r3.0"] = System(random_sequential(1000, 0.5, 0.8, seed=36), 1.0, 3.0)
+    out["long_rows_r6.5"] = System(simple_cubic_random(14, 14, 14, seed=37), 1.0, 6.5)  # > 1024 per row
+    return out
+
+
+@pytest.mark.parametrize("name", list(_cell_systems()))
+def test_cell_list_csr_bitwise(oracle, name):
+    """The cell-list CSR build (O(N z)) gives the reference's O(N^2) scan exactly: the same
+    row lengths, columns in the same order and bit-identical values."""
+    s = _cell_systems()[name]
+    ptr, cols, vals = s.csr()
+    optr, ocols, ovals = oracle.csr(s)
+    assert np.array_equal(ptr.astype(np.uint64), optr)
+    assert np.array_equal(cols.astype(np.uint64), ocols)
+    assert same_double(vals, ovals)
+
+
 @pytest.mark.parametrize("precision,rtol", [("fp32", 2.0 ** -24), ("bf16", 2.0 ** -8)])
 def test_low_precision_couplings(precision, rtol):
     s = _systems()[3]
