@@ -23,10 +23,12 @@
 //   field and spin when it becomes the site: fma(m, J, f) with m = +-2 rounds the reference's
 //   f + m*J once.
 // * At the end of an attempt, after its stores, the warp copies the next site's neighbour
-//   fields into its slot (speculatively: a rejected flip discards them) before the next
-//   acceptance log; the next attempt decides and on acceptance stores
+//   fields into its slot (speculatively: a rejected flip discards them); the next attempt
+//   decides and on acceptance stores
 //   fields[c] = fma(m, J_ic, fields[c]) for every neighbour c.  Each field changes at most
 //   once per flip, so the order of the neighbour updates is immaterial.
+// * The draws are generated 32 at a time, lane j keeping draw j with its site and the log
+//   of its uniform, so the acceptance log is off the attempt's chain.
 // * All 32 lanes evaluate the decision chain redundantly; histogram increments go to a
 //   32-bit shared-memory delta per bin that is folded into H at the end of the batch, and the
 //   Wang-Landau count of active bins is updated once from the visited mask, as in the dense
@@ -231,18 +233,45 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
 
     // Slots o, o+1, o+2 (mod 4) hold the site of the next attempt (draw hq) and the candidates
     // (draws hq+1, hq+2); site indices i0, i1, i2.
+    // The draws come in batches of 32: every lane steps the generator through the batch and
+    // keeps draw j = lane, with its site and log(max(u, 2^-53)) (src/wang_landau.cpp:250, 261);
+    // an attempt reads them from the owning lane.  Two batches are held: draws [first, first+64).
     Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};
+    auto generate = [&](int& site, double& log_u) {
+        uint64_t mine = 0;
+#pragma unroll 4
+        for (int j = 0; j < 32; ++j) {
+            const uint64_t d = rng.next();
+            mine = lane == j ? d : mine;
+        }
+        site = site_of(mine);
+        log_u = log(fmax(to_uniform(mine), 0x1.0p-53));
+    };
+    uint32_t first = 0, hq = 0;  // draw index of lane 0 of the first batch; of the current site
+    int site_a, site_b;
+    double lnu_a, lnu_b;
+    generate(site_a, lnu_a);
+    generate(site_b, lnu_b);
+    auto draw_site = [&](uint32_t k) { return __shfl_sync(kFull, k < first + 32 ? site_a : site_b, k & 31); };
+    auto draw_lnu = [&](uint32_t k) { return __shfl_sync(kFull, k < first + 32 ? lnu_a : lnu_b, k & 31); };
     int o = 0;
-    int i0 = site_of(rng.next());
-    uint64_t d1 = rng.next(), d2 = rng.next();
-    int i1 = site_of(d1), i2 = site_of(d2);
+    int i0 = draw_site(0), i1 = draw_site(1), i2 = draw_site(2);
     fetch(0, i0);
     fetch(1, i1);
     fetch(2, i2);
     cp_wait<0>();
     __syncwarp();
     load_neighbours(0);
-    double lnu = log(fmax(to_uniform(d1), 0x1.0p-53));
+    double lnu = draw_lnu(1);
+    // after the site moved to draw hq: keep hq+4 inside the two batches
+    auto advance_batches = [&]() {
+        if (hq >= first + 32) {
+            site_a = site_b;
+            lnu_a = lnu_b;
+            first += 32;
+            generate(site_b, lnu_b);
+        }
+    };
 
     // The attempts of one batch; kIT selects the 1/t stage (per-attempt factor and active
     // count) or the Wang-Landau / frozen stages (constant factor).
@@ -253,17 +282,17 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
         if (kIT && active_count != 0) factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + 1);
         for (uint32_t t = 0; t < batch;) {
             if (i0 < 0) {  // rare: bounded() rejects draw hq; the next draw is the site
-                d1 = d2;
-                d2 = rng.next();
+                hq += 1;
+                advance_batches();
                 i0 = i1;
                 i1 = i2;
-                i2 = site_of(d2);
+                i2 = draw_site(hq + 2);
                 fetch(o + 3, i2);
                 o = (o + 1) & (kCsrSlots - 1);
                 cp_wait<2>();  // the new site's row (an older group) has landed
                 __syncwarp();
                 load_neighbours(o);
-                lnu = log(fmax(to_uniform(d1), 0x1.0p-53));
+                lnu = draw_lnu(hq + 1);
                 continue;
             }
             // the decision (attempt_flip, src/wang_landau.cpp:244-262)
@@ -333,28 +362,28 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
 
             __syncwarp();  // this attempt's stores and reads of the slots precede later copies
             if (need_u) {  // draw hq+1 was the uniform: the site is draw hq+2
-                d1 = rng.next();
-                d2 = rng.next();
+                hq += 2;
+                advance_batches();
                 i0 = i2;
-                i1 = site_of(d1);
-                i2 = site_of(d2);
+                i1 = draw_site(hq + 1);
+                i2 = draw_site(hq + 2);
                 fetch(o + 3, i1);
                 fetch(o + 4, i2);  // the slot of the site just done
                 o = (o + 2) & (kCsrSlots - 1);
                 cp_wait<3>();  // the new site's row (older than the last three groups) has landed
             } else {
-                d1 = d2;
-                d2 = rng.next();
+                hq += 1;
+                advance_batches();
                 i0 = i1;
                 i1 = i2;
-                i2 = site_of(d2);
+                i2 = draw_site(hq + 2);
                 fetch(o + 3, i2);
                 o = (o + 1) & (kCsrSlots - 1);
                 cp_wait<2>();
             }
             __syncwarp();
-            load_neighbours(o);  // issued before the log below, so that its latency overlaps it
-            lnu = log(fmax(to_uniform(d1), 0x1.0p-53));
+            load_neighbours(o);
+            lnu = draw_lnu(hq + 1);
         }
     };
     if (stage == kInverseTime)
@@ -363,10 +392,8 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
         run(std::false_type{});
     cp_wait<0>();  // no copy is in flight when the walker leaves
 
-    // the generator is three draws past the last consumed one (the next site, hq+1, hq+2)
-    rng_step_back(rng);
-    rng_step_back(rng);
-    rng_step_back(rng);
+    // the generator is at draw first+64; step back to the last consumed draw, hq-1
+    for (uint32_t k = hq; k != first + 64; ++k) rng_step_back(rng);
     if (lane == 0) lg_s[cur - wb] = lg_cur;
     __syncwarp();
     uint64_t active_after = 0;
