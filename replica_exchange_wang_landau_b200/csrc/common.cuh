@@ -303,6 +303,7 @@ struct EngineView {
     const double* ell_val64;       // FP64 couplings (FP64 runs)
     const float* ell_val32;        // FP32 couplings (FP32 runs)
     int32_t ell_width;             // 32, 64, 128 or 256; 0 when not built
+    int32_t spins_global;          // the generic sweep and the initialisation read spins from HBM
     Grid grid;
     int32_t walkers;
     int32_t walkers_per_window;

@@ -255,7 +255,10 @@ void Engine::initialise_walkers(const wlg_run_config& c) {
     v.p = p_;
     v.ctl = d_ctl_.get<Control>();
 
+    v.spins_global = 0;
     smem_fields_ = !sys_.csr || fields_fit_in_smem(v, features_);
+    // a large cutoff system keeps the spins of the initialisation and the generic sweep in HBM
+    if (sys_.csr && !smem_fields_ && walker_smem_bytes(v, false, features_) > 200 * 1024) v.spins_global = 1;
     if (!sys_.csr && !fields_fit_in_smem(v, features_))
         throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Dense system too large for the shared-memory walker (use a cutoff)");
 

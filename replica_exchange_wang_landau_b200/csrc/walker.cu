@@ -139,7 +139,7 @@ __device__ __forceinline__ double warp_total_energy(const EngineView& v, const i
 // ---- shared-memory carve-up ---------------------------------------------------------------
 
 size_t walker_smem_bytes(const EngineView& v, bool smem_fields, bool features) {
-    return smem_layout(v.ld, v.max_window_bins, smem_fields, features).total;
+    return smem_layout(v.ld, v.max_window_bins, smem_fields, features, v.spins_global == 0).total;
 }
 
 bool fields_fit_in_smem(const EngineView& v, bool features) {
@@ -159,13 +159,12 @@ __global__ void __launch_bounds__(256) walk_kernel(EngineView v, WalkArgs a) {
     Control* ctl = v.ctl;
     if (a.epoch_mode && *reinterpret_cast<volatile int32_t*>(&ctl->done)) return;
 
-    const SmemLayout L = smem_layout(v.ld, v.max_window_bins, kSmemF, kFeat);
+    const SmemLayout L = smem_layout(v.ld, v.max_window_bins, kSmemF, kFeat, v.spins_global == 0);
     unsigned char* base = smem + static_cast<size_t>(warp) * a.smem_per_walker;
     double* lg_s = reinterpret_cast<double*>(base + L.log_g);
     uint64_t* h_s = reinterpret_cast<uint64_t*>(base + L.hist);
     double* sq_s = reinterpret_cast<double*>(base + L.sq);
     uint64_t* ds_s = reinterpret_cast<uint64_t*>(base + L.ds);
-    int8_t* sp_s = reinterpret_cast<int8_t*>(base + L.spins);
     uint8_t* act_s = base + L.active;
     uint8_t* ref_s = base + L.refine;
 
@@ -174,6 +173,7 @@ __global__ void __launch_bounds__(256) walk_kernel(EngineView v, WalkArgs a) {
     const size_t boff = static_cast<size_t>(w) * static_cast<size_t>(v.grid.count) + static_cast<size_t>(wb);
     double* fg = v.fields + static_cast<size_t>(st.slot) * v.ld;
     int8_t* sg = v.spins + static_cast<size_t>(st.slot) * v.ld;
+    int8_t* sp_s = v.spins_global ? sg : reinterpret_cast<int8_t*>(base + L.spins);
     double* f = kSmemF ? reinterpret_cast<double*>(base + L.fields) : fg;
     const DeviceParams& P = v.p;
     const bool collect = kFeat && P.collect;
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(256) walk_kernel(EngineView v, WalkArgs a) {
         double2* dst = reinterpret_cast<double2*>(f);
         for (int k = lane; k < (v.ld >> 1); k += 32) dst[k] = src[k];
     }
-    {
+    if (!v.spins_global) {
         const int4* src = reinterpret_cast<const int4*>(sg);
         int4* dst = reinterpret_cast<int4*>(sp_s);
         for (int k = lane; k < (v.ld >> 4); k += 32) dst[k] = src[k];
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(256) walk_kernel(EngineView v, WalkArgs a) {
         double2* dst = reinterpret_cast<double2*>(fg);
         for (int k = lane; k < (v.ld >> 1); k += 32) dst[k] = src[k];
     }
-    {
+    if (!v.spins_global) {
         const int4* src = reinterpret_cast<const int4*>(sp_s);
         int4* dst = reinterpret_cast<int4*>(sg);
         for (int k = lane; k < (v.ld >> 4); k += 32) dst[k] = src[k];
@@ -390,11 +390,11 @@ __global__ void __launch_bounds__(256) init_kernel(EngineView v, InitArgs a) {
     const int w = blockIdx.x * (blockDim.x >> 5) + warp;
     if (w >= v.walkers) return;
 
-    const SmemLayout L = smem_layout(v.ld, v.max_window_bins, kSmemF, kFeat);
+    const SmemLayout L = smem_layout(v.ld, v.max_window_bins, kSmemF, kFeat, v.spins_global == 0);
     unsigned char* base = smem + static_cast<size_t>(warp) * a.smem_per_walker;
-    int8_t* s = reinterpret_cast<int8_t*>(base + L.spins);
     double* fg = v.fields + static_cast<size_t>(w) * v.ld;
     int8_t* sg = v.spins + static_cast<size_t>(w) * v.ld;
+    int8_t* s = v.spins_global ? sg : reinterpret_cast<int8_t*>(base + L.spins);
     double* f = kSmemF ? reinterpret_cast<double*>(base + L.fields) : fg;
 
     WalkerState st = v.ws[w];  // window, slot and zeroed counters prepared by the host
@@ -524,7 +524,8 @@ __global__ void __launch_bounds__(256) init_kernel(EngineView v, InitArgs a) {
     }
     if constexpr (kSmemF)
         for (int i = lane; i < v.ld; i += 32) fg[i] = f[i];
-    for (int i = lane; i < v.ld; i += 32) sg[i] = s[i];
+    if (!v.spins_global)
+        for (int i = lane; i < v.ld; i += 32) sg[i] = s[i];
     if (lane == 0) v.ws[w] = st;
 }
 

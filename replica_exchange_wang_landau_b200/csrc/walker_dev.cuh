@@ -164,7 +164,8 @@ struct SmemLayout {
     size_t fields, log_g, hist, sq, ds, spins, active, refine, total;
 };
 
-__host__ __device__ inline SmemLayout smem_layout(int ld, int mwb, bool smem_fields, bool features) {
+__host__ __device__ inline SmemLayout smem_layout(int ld, int mwb, bool smem_fields, bool features,
+                                                  bool smem_spins = true) {
     SmemLayout L;
     size_t at = 0;
     L.fields = at; at += smem_fields ? static_cast<size_t>(ld) * 8 : 0;
@@ -172,7 +173,7 @@ __host__ __device__ inline SmemLayout smem_layout(int ld, int mwb, bool smem_fie
     L.hist = at; at += round16(static_cast<size_t>(mwb) * 8);
     L.sq = at; at += features ? round16(static_cast<size_t>(mwb) * 8) : 0;
     L.ds = at; at += features ? round16(static_cast<size_t>(mwb) * 8) : 0;
-    L.spins = at; at += round16(static_cast<size_t>(ld));
+    L.spins = at; at += smem_spins ? round16(static_cast<size_t>(ld)) : 0;
     L.active = at; at += round16(static_cast<size_t>(mwb));
     L.refine = at; at += features ? round16(static_cast<size_t>(mwb)) : 0;
     L.total = at;

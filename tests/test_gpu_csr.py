@@ -123,3 +123,26 @@ def test_csr_32cubed_fields_consistent(precision):
             lo, hi = e.window(w // c.walkers)
             b = int(np.floor((snap.energy - c.emin) / c.bin_width))
             assert lo <= b < hi
+
+
+@pytest.mark.parametrize("collect", [False, True])
+def test_csr_large_system_spins_in_hbm(collect):
+    """60^3 lattice (N = 216000), cutoff 1.5: the walkers' spins no longer fit in shared memory
+    next to their window, so the initialisation and the generic sweep (pilot statistics) read
+    them from HBM; the fields the sweep maintains still equal a full recompute."""
+    g = Geometry.simple_cubic(60, 60, 60, 1.0, (0.0, 0.0, 1.0), True)
+    s = System(g, 1.0, 1.5)
+    c = RunConfig(emin=-20000.0, emax=20000.0, bin_width=100.0, windows=1, walkers=2, seed=7)
+    c.wl = WlParameters(0.8, 100, 1e-8, 1000, 0, True, collect_window_statistics=collect)
+    c.exchange_interval_mcs = 0.01
+    c.resolve_mcs(s.size())
+    with Engine(s, c) as e:
+        e.run_epochs(3)
+        t = e.totals()
+        assert t["attempted"] == 3 * 2 * c.exchange_interval_attempts
+        assert 0 < t["accepted"]
+        for w in range(e.walkers):
+            snap = e.snapshot(w)
+            fields, energy = s.local_fields(snap.spins)
+            assert np.max(np.abs(snap.fields - fields)) <= 1e-9
+            assert abs(snap.energy - energy) <= 1e-6
