@@ -29,6 +29,9 @@
 //   once per flip, so the order of the neighbour updates is immaterial.
 // * The draws are generated 32 at a time, lane j keeping draw j with its site and the log
 //   of its uniform, so the acceptance log is off the attempt's chain.
+// * With pilot statistics on (an adaptive-window pilot), lane 0 adds each attempt's squared
+//   displacement and sample to the old bin, and an accepted flip updates the round-trip state
+//   and the representative configurations, in the reference's order.
 // * All 32 lanes evaluate the decision chain redundantly; histogram increments go to a
 //   32-bit shared-memory delta per bin that is folded into H at the end of the batch, and the
 //   Wang-Landau count of active bins is updated once from the visited mask, as in the dense
@@ -65,14 +68,17 @@ __host__ __device__ inline CsrSlot csr_slot(int width, int vbytes) {
 constexpr int kCsrSlots = 4;
 
 struct CsrSweepLayout {
-    size_t slots, log_g, hist, hd, active, total;
+    size_t slots, log_g, hist, sq, ds, hd, active, total;
 };
-__host__ __device__ inline CsrSweepLayout csr_sweep_layout(int mwb, int width, int vbytes) {
+// `collect`: the pilot statistics of the window (squared displacements, sample counts)
+__host__ __device__ inline CsrSweepLayout csr_sweep_layout(int mwb, int width, int vbytes, bool collect) {
     CsrSweepLayout L;
     size_t at = 0;
     L.slots = at; at += kCsrSlots * csr_slot(width, vbytes).bytes;
     L.log_g = at; at += round16(static_cast<size_t>(mwb) * 8);
     L.hist = at; at += round16(static_cast<size_t>(mwb) * 8);
+    L.sq = at; at += collect ? round16(static_cast<size_t>(mwb) * 8) : 0;
+    L.ds = at; at += collect ? round16(static_cast<size_t>(mwb) * 8) : 0;
     L.hd = at; at += round16(static_cast<size_t>(mwb) * 4);
     L.active = at; at += round16(static_cast<size_t>(mwb));
     L.total = at;
@@ -104,7 +110,7 @@ __device__ __forceinline__ const typename EllValue<kPrec>::T* ell_values(const E
     else return v.ell_val64;
 }
 
-template <int kK, bool kPow2, int kPrec>
+template <int kK, bool kPow2, int kPrec, bool kCollect>
 __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArgs a) {
     using VT = typename EllValue<kPrec>::T;
     constexpr int kWidth = 32 * kK;
@@ -116,7 +122,7 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
     Control* ctl = v.ctl;
     if (a.epoch_mode && *reinterpret_cast<volatile int32_t*>(&ctl->done)) return;
 
-    const CsrSweepLayout L = csr_sweep_layout(v.max_window_bins, kWidth, sizeof(VT));
+    const CsrSweepLayout L = csr_sweep_layout(v.max_window_bins, kWidth, sizeof(VT), kCollect);
     const CsrSlot S = csr_slot(kWidth, sizeof(VT));
     unsigned char* base = smem + static_cast<size_t>(warp) * L.total;
     unsigned char* ring = base + L.slots;
@@ -125,6 +131,8 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
     uint64_t* h_s = reinterpret_cast<uint64_t*>(base + L.hist);
     uint32_t* hd = reinterpret_cast<uint32_t*>(base + L.hd);
     uint8_t* act_s = base + L.active;
+    double* sq_s = reinterpret_cast<double*>(base + L.sq);
+    uint64_t* ds_s = reinterpret_cast<uint64_t*>(base + L.ds);
 
     WalkerState st = v.ws[w];
     const int wb = v.win_begin[st.window], we = v.win_end[st.window], nbins = we - wb;
@@ -154,8 +162,20 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
         h_s[b] = v.hist[boff + b];
         act_s[b] = v.active[boff + b];
         hd[b] = 0;
+        if constexpr (kCollect) {
+            sq_s[b] = v.sqdisp[boff + b];
+            ds_s[b] = v.dsamples[boff + b];
+        }
     }
     __syncwarp();
+    // pilot statistics (src/wang_landau.cpp:272-276, 317-342): round trips and representatives
+    const double lower = window_lower(v, wb), upper = window_lower(v, we);
+    int32_t rt_state = st.rt_state;
+    uint64_t trips = st.round_trips;
+    if (kCollect && st.rep_pending) {  // a replica exchange changed the configuration
+        warp_update_representatives(v, w, st.energy, sg, lane);
+        st.rep_pending = 0;
+    }
 
     auto site_of = [&](uint64_t d) -> int { return d < fm.threshold ? -1 : static_cast<int>(fast_mod(fm, d)); };
     auto slot_ptr = [&](int k) { return ring + static_cast<size_t>(k & (kCsrSlots - 1)) * S.bytes; };
@@ -333,6 +353,11 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
             n_acc += accepted ? 1u : 0u;
             n_forced += (accepted && forced) ? 1u : 0u;
             ++t;
+            if (kCollect && lane == 0) {  // the displacement out of the old bin, 0 when rejected
+                const double displacement = accepted ? m * slot_field(o) : 0.0;
+                sq_s[cur - wb] += displacement * displacement;
+                ++ds_s[cur - wb];
+            }
 
             // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
             if (kIT && stage == kInverseTime) {
@@ -361,6 +386,10 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
             }
 
             __syncwarp();  // this attempt's stores and reads of the slots precede later copies
+            if (kCollect && accepted) {
+                round_trip_update(E, lower, upper, P.round_trip_margin, rt_state, trips);
+                warp_update_representatives(v, w, E, sg, lane);
+            }
             if (need_u) {  // draw hq+1 was the uniform: the site is draw hq+2
                 hq += 2;
                 advance_batches();
@@ -418,6 +447,8 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
     st.last_accepted = st.attempted - since;
     st.active_count = active_count;
     st.cur_bin = cur;
+    st.rt_state = rt_state;
+    st.round_trips = trips;
 
     if (a.epoch_mode && st.stage == kWangLandau) {
         const bool at_limit = P.max_attempts != 0 && st.attempted >= P.max_attempts;
@@ -432,6 +463,10 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
         v.log_g[boff + b] = lg_s[b];
         v.hist[boff + b] = h_s[b];
         v.active[boff + b] = act_s[b];
+        if constexpr (kCollect) {
+            v.sqdisp[boff + b] = sq_s[b];
+            v.dsamples[boff + b] = ds_s[b];
+        }
     }
     if (lane == 0) {
         v.ws[w] = st;
@@ -444,27 +479,37 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
 
 using SweepFn = void (*)(EngineView, WalkArgs);
 
-template <int kK, bool kPow2, int kPrec>
+template <int kK, bool kPow2, int kPrec, bool kCollect>
 SweepFn csr_fn() {
     static bool configured = false;
     if (!configured) {
-        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_csr_kernel<kK, kPow2, kPrec>),
+        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_csr_kernel<kK, kPow2, kPrec, kCollect>),
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
                    "cudaFuncSetAttribute");
         configured = true;
     }
-    return &sweep_csr_kernel<kK, kPow2, kPrec>;
+    return &sweep_csr_kernel<kK, kPow2, kPrec, kCollect>;
 }
 
-template <bool kPow2, int kPrec>
+template <bool kPow2, int kPrec, bool kCollect>
 SweepFn pick_csr_width(int width) {
     switch (width) {
-        case 32: return csr_fn<1, kPow2, kPrec>();
-        case 64: return csr_fn<2, kPow2, kPrec>();
-        case 128: return csr_fn<4, kPow2, kPrec>();
-        case 256: return csr_fn<8, kPow2, kPrec>();
+        case 32: return csr_fn<1, kPow2, kPrec, kCollect>();
+        case 64: return csr_fn<2, kPow2, kPrec, kCollect>();
+        case 128: return csr_fn<4, kPow2, kPrec, kCollect>();
+        case 256: return csr_fn<8, kPow2, kPrec, kCollect>();
         default: return nullptr;
     }
+}
+
+template <bool kCollect>
+SweepFn pick_csr(const EngineView& v) {
+    const bool pow2 = v.grid.pow2_width != 0;
+    if (v.precision == WLG_PRECISION_FP32)
+        return pow2 ? pick_csr_width<true, WLG_PRECISION_FP32, kCollect>(v.ell_width)
+                    : pick_csr_width<false, WLG_PRECISION_FP32, kCollect>(v.ell_width);
+    return pow2 ? pick_csr_width<true, WLG_PRECISION_FP64, kCollect>(v.ell_width)
+                : pick_csr_width<false, WLG_PRECISION_FP64, kCollect>(v.ell_width);
 }
 
 }  // namespace
@@ -501,16 +546,12 @@ void launch_ell_fill(int n, int width, const int32_t* ptr, const int32_t* col, c
 }
 
 bool launch_sweep_csr(const EngineView& v, const WalkArgs& a, int walkers_per_block, cudaStream_t stream) {
-    if (!v.csr || v.ell_width == 0 || v.p.collect || v.p.nalivaiko) return false;
-    const bool pow2 = v.grid.pow2_width != 0;
-    SweepFn fn = v.precision == WLG_PRECISION_FP32
-                     ? (pow2 ? pick_csr_width<true, WLG_PRECISION_FP32>(v.ell_width)
-                             : pick_csr_width<false, WLG_PRECISION_FP32>(v.ell_width))
-                     : (pow2 ? pick_csr_width<true, WLG_PRECISION_FP64>(v.ell_width)
-                             : pick_csr_width<false, WLG_PRECISION_FP64>(v.ell_width));
+    if (!v.csr || v.ell_width == 0 || v.p.nalivaiko) return false;  // the Nalivaiko mask: walk_kernel
+    const bool collect = v.p.collect != 0;
+    SweepFn fn = collect ? pick_csr<true>(v) : pick_csr<false>(v);
     if (!fn) return false;
     const int vbytes = v.precision == WLG_PRECISION_FP32 ? 4 : 8;
-    const size_t per_walker = csr_sweep_layout(v.max_window_bins, v.ell_width, vbytes).total;
+    const size_t per_walker = csr_sweep_layout(v.max_window_bins, v.ell_width, vbytes, collect).total;
     if (per_walker > 227 * 1024) return false;
     int wpb = walkers_per_block < 1 ? 1 : (walkers_per_block > 8 ? 8 : walkers_per_block);
     while (wpb > 1 && per_walker * static_cast<size_t>(wpb) > 227 * 1024) --wpb;

@@ -15,8 +15,9 @@ from replica_exchange_wang_landau_b200.geometry import simple_cubic_random
 pytestmark = pytest.mark.gpu
 
 
-def test_adaptive_pilot_matches_reference(reference):
-    s = System(simple_cubic_random(4, 4, 4, seed=3, periodic=True), 1.0, 0.0)
+@pytest.mark.parametrize("cutoff", [0.0, 2.0])  # dense couplings; CSR (the CSR sweep with pilot statistics)
+def test_adaptive_pilot_matches_reference(reference, cutoff):
+    s = System(simple_cubic_random(4, 4, 4, seed=3, periodic=True), 1.0, cutoff)
     c = RunConfig(emin=-60, emax=60, bin_width=0.5, windows=3, walkers=2, overlap=0.5, seed=17)
     c.wl = WlParameters(0.8, 100, 1e-3, 1000, 0, True)
     c.exchange_interval_mcs = 1.0

@@ -80,6 +80,15 @@ RUNS = {
                          dict(emin=-120, emax=60, bin_width=0.5, windows=2, walkers=2, seed=43, max_mcs=400,
                               exchange_interval_mcs=1, check_interval_mcs=5),
                          dict(flatness=0.3, minimum_visits=3, final_factor=1e-4)),
+    # pilot statistics: squared displacements, samples, round trips and representatives
+    "z80_pilot": (lambda: _lattice((6, 6, 6), 21, 2.5),
+                  dict(emin=-200, emax=100, bin_width=0.75, windows=3, walkers=2, seed=44, max_mcs=60,
+                       exchange_interval_mcs=0.5, check_interval_mcs=2),
+                  dict(collect_window_statistics=True, final_factor=1e-2)),
+    "z178_pilot": (lambda: _lattice((8, 8, 8), 22, 3.5),
+                   dict(emin=-300, emax=100, bin_width=1.0, windows=2, walkers=3, seed=45, max_mcs=30,
+                        exchange_interval_mcs=1, check_interval_mcs=2),
+                   dict(collect_window_statistics=True, final_factor=1e-2)),
 }
 
 
