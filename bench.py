@@ -279,7 +279,7 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
             line["cpu_baseline"] = cpu
         if world == 1 and not args.skip_extras:
             try:
-                line["mixed_precision"] = mixed_precision_lines(min(epochs, 30))
+                line["mixed_precision"] = mixed_precision_lines()
             except Exception as exc:  # reported, never fatal to the headline line
                 line["mixed_precision"] = {"error": str(exc)}
             try:
@@ -293,25 +293,72 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
         print(json.dumps(line))
 
 
-def mixed_precision_lines(epochs: int) -> dict:
-    """The same workload with FP32 and BF16 (+ row scale) couplings: device attempts/s of the
-    sweeps and the drift that the periodic FP64 recompute (every 10 MCS) measured."""
+def _pilot_range(J: np.ndarray, mcs: int, seed: int) -> tuple:
+    """wl_run --pilot (apps/wl_run.cpp:84-100) restated: an infinite-temperature walk (every
+    single-spin flip accepted) from all spins up, then the visited range padded by 5% each side."""
+    n = J.shape[0]
+    rng = np.random.default_rng(seed)
+    s = np.ones(n)
+    h = J @ s
+    e = 0.5 * float(s @ h)
+    lo = hi = e
+    for i in rng.integers(0, n, size=mcs * n):
+        e += -2.0 * s[i] * h[i]
+        h -= 2.0 * s[i] * J[i]
+        s[i] = -s[i]
+        lo, hi = min(lo, e), max(hi, e)
+    pad = max(1e-12, 0.05 * (hi - lo))
+    return lo - pad, hi + pad
+
+
+def mixed_precision_workload(precisions=("fp64", "fp32", "bf16")):
+    """The mixed-precision configuration: a 16x16x16 simple cubic lattice with 40% of the sites
+    removed (seeded; N = 2458), slab geometry periodic in x and y (box 16, 16, 0), random-sphere
+    axes, dense couplings; 32 windows x 8 walkers at 75% overlap, exchange and FP64 recompute
+    every MCS.  The grid is the pilot range of a 100-MCS infinite-temperature walk (the
+    reference's pilot, seeded here; its runs use longer walks), in bins of 0.5."""
+    from replica_exchange_wang_landau_b200.engine import RunConfig, System
+    from replica_exchange_wang_landau_b200.geometry import diluted_cubic
+    g = diluted_cubic(16, 16, 16, 0.4, seed=1, periodic=True, box=(16.0, 16.0, 0.0))
+    system = System(g, 1.0, 0.0)
+    lo, hi = _pilot_range(system.couplings("fp64"), 100, seed=1)
+    width = 0.5
+    emin, emax = width * np.floor(lo / width), width * np.ceil(hi / width)
+    configs = {}
+    for precision in precisions:
+        config = RunConfig(emin=float(emin), emax=float(emax), bin_width=width, windows=32, walkers=8,
+                           overlap=0.75, seed=1, exchange_interval_mcs=1.0)
+        config.coupling_precision = precision
+        config.recompute_interval_mcs = 1.0
+        config.resolve_mcs(system.size())
+        configs[precision] = config
+    return system, configs
+
+
+def mixed_precision_lines(epochs: int = 10) -> dict:
+    """The mixed-precision configuration with FP64, FP32 and BF16 (+ FP32 row scale) couplings:
+    device attempts/s of the product path (sweeps, exchanges and, for FP32 / BF16, the FP64
+    recompute and resync after every epoch) and the drift the recompute measured."""
     from replica_exchange_wang_landau_b200.engine import Engine
     out = {}
-    for precision in ("fp32", "bf16"):
-        system, config = make_workload(seed=1)
-        config.coupling_precision = precision
-        config.recompute_interval_mcs = 10.0
+    system, configs = mixed_precision_workload()
+    for precision, config in configs.items():
+        t0 = time.perf_counter()
         with Engine(system, config) as eng:
-            eng.run_epochs(3)
-            t = eng.time_epochs(epochs)
-            eng.run_epochs(epochs)
+            create_s = time.perf_counter() - t0
+            eng.time_run(2)
+            t = eng.time_run(epochs)
             rep = eng.precision_report()
-        out[precision] = {"value": t["attempted"] / (t["total_ms"] / 1e3), "unit": UNIT,
-                          "epochs_timed": t["epochs"], "recompute_interval_mcs": 10.0,
+        out[precision] = {"value": t["attempted"] / (t["total_ms"] / 1e3), "unit": UNIT, "epochs_timed": t["epochs"],
+                          "ms_per_epoch": t["total_ms"] / max(1, t["epochs"]),
+                          "recompute_interval_mcs": 1.0 if precision != "fp64" else None,
                           "recomputes": rep["recomputes"], "max_field_drift": rep["max_field_drift"],
                           "max_energy_drift": rep["max_energy_drift"], "deferred": rep["deferred"],
-                          "bin_changes": rep["bin_changes"]}
+                          "bin_changes": rep["bin_changes"], "engine_create_s": create_s,
+                          "acceptance": t["accepted"] / max(1, t["attempted"])}
+    out["workload"] = ("16x16x16 simple cubic, 40% of sites removed (seed 1, N = 2458), slab box (16, 16, 0), "
+                       "random-sphere axes, dense J; 32 windows x 8 walkers, exchange and FP64 recompute every MCS; "
+                       f"grid [{config.emin:g}, {config.emax:g}] in bins of {config.bin_width:g}")
     return out
 
 
@@ -481,11 +528,16 @@ def main() -> None:
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-extras", action="store_true",
                     help="skip the mixed-precision lines and the learned-vs-plain time to accuracy")
+    ap.add_argument("--mixed-only", action="store_true",
+                    help="print only the mixed-precision configuration's lines (N = 2458, FP64 / FP32 / BF16)")
     ap.add_argument("--csr-only", action="store_true",
                     help="print only the CSR configuration's line (the 32^3 lattice, 1024 walkers)")
     args = ap.parse_args()
     if args.csr_only:
         print(json.dumps({"csr_batched": csr_batched_line()}))
+        return
+    if args.mixed_only:
+        print(json.dumps({"mixed_precision": mixed_precision_lines()}))
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

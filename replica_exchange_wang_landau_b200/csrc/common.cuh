@@ -259,7 +259,7 @@ struct alignas(16) Control {
 struct PrecisionReport {
     unsigned long long max_field_drift_bits;   // max |h - h64| (bits of a non-negative double)
     unsigned long long max_energy_drift_bits;  // max |E - E64|
-    unsigned long long recomputes;             // recompute passes (host-counted)
+    unsigned long long recomputes;             // recompute passes applied
     unsigned long long resynced;               // walker resyncs applied
     unsigned long long deferred;               // resyncs deferred: E64 outside the window
     unsigned long long bin_changes;            // resyncs that moved the current bin

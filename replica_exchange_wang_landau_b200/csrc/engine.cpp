@@ -428,10 +428,7 @@ void Engine::build_graph() {
     check_cuda(cudaStreamSynchronize(stream_), "sync");
     check_cuda(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
-        for (int e = 0; e < epochs_per_graph; ++e) {
-            launch_walk(view_, a, walkers_per_block, stream_);
-            launch_exchange(view_, stream_);
-        }
+        for (int e = 0; e < epochs_per_graph; ++e) launch_epoch(a);
     } catch (...) {
         cudaGraph_t g = nullptr;
         cudaStreamEndCapture(stream_, &g);
@@ -453,23 +450,16 @@ void Engine::launch_epochs(uint64_t count) {
     if (count == static_cast<uint64_t>(epochs_per_graph) && epochs_per_graph > 1) {
         // first use primes the kernel attributes outside of capture
         if (!graph_exec_) {
-            launch_walk(view_, a, walkers_per_block, stream_);
-            launch_exchange(view_, stream_);
+            launch_epoch(a);
             count -= 1;
             build_graph();
-            for (uint64_t e = 0; e < count; ++e) {
-                launch_walk(view_, a, walkers_per_block, stream_);
-                launch_exchange(view_, stream_);
-            }
+            for (uint64_t e = 0; e < count; ++e) launch_epoch(a);
             return;
         }
         check_cuda(cudaGraphLaunch(graph_exec_, stream_), "graph launch");
         return;
     }
-    for (uint64_t e = 0; e < count; ++e) {
-        launch_walk(view_, a, walkers_per_block, stream_);
-        launch_exchange(view_, stream_);
-    }
+    for (uint64_t e = 0; e < count; ++e) launch_epoch(a);
 }
 
 void Engine::maybe_checkpoint() {
@@ -547,7 +537,7 @@ void Engine::run_epochs(uint64_t max_epochs, uint64_t* epochs_run, int32_t* done
             const uint64_t epochs_needed = std::max<uint64_t>(1, (need + p_.exchange_interval - 1) / p_.exchange_interval);
             chunk = std::min(chunk, epochs_needed);
         }
-        if (recompute_epochs_) chunk = std::min(chunk, std::max<uint64_t>(1, next_recompute_ - epochs_));
+        if (recompute_epochs_ > 1) chunk = std::min(chunk, std::max<uint64_t>(1, next_recompute_ - epochs_));
         launch_epochs(chunk);
         budget -= std::min(budget, chunk);
         after_epochs();
@@ -559,13 +549,25 @@ void Engine::run_epochs(uint64_t max_epochs, uint64_t* epochs_run, int32_t* done
 
 // The FP64 recompute of a mixed-precision run: all configurations' fields and energies from
 // the FP64 J (reference summation order), then the per-walker drift measurement and resync.
-void Engine::recompute_fields() {
+// Stream-ordered, no host synchronisation: a recompute every epoch is part of the epoch graph.
+void Engine::launch_recompute() {
     compute_fields(view_, d_spins_.get<int8_t>(), static_cast<int64_t>(sys_.ld), d_rfields_.get<double>(),
                    static_cast<int64_t>(sys_.ld), d_renergy_.get<double>(), static_cast<int>(walkers_), stream_);
     launch_resync(view_, d_rfields_.get<double>(), d_renergy_.get<double>(), d_prec_.get<PrecisionReport>(),
                   stream_);
-    ++recomputes_;
+}
+
+void Engine::recompute_fields() {
+    launch_recompute();
     check_device_error();
+}
+
+// One epoch of run_rewl on the stream: the sweep, the exchange and, when the recompute
+// interval is one epoch, the FP64 recompute.
+void Engine::launch_epoch(const WalkArgs& a) {
+    launch_walk(view_, a, walkers_per_block, stream_);
+    launch_exchange(view_, stream_);
+    if (recompute_epochs_ == 1) launch_recompute();
 }
 
 void Engine::precision_report(wlg_precision_report* out) {
@@ -575,7 +577,7 @@ void Engine::precision_report(wlg_precision_report* out) {
     *out = wlg_precision_report{};
     out->coupling_precision = precision_;
     out->recompute_interval_attempts = recompute_epochs_ ? cfg_.recompute_interval_attempts : 0;
-    out->recomputes = recomputes_;
+    out->recomputes = r.recomputes;
     out->resynced = r.resynced;
     out->deferred = r.deferred;
     out->bin_changes = r.bin_changes;
@@ -587,7 +589,7 @@ void Engine::precision_report(wlg_precision_report* out) {
 // and the progress line.
 void Engine::after_epochs() {
     check_device_error();
-    if (recompute_epochs_ && !done_ && epochs_ >= next_recompute_) {
+    if (recompute_epochs_ > 1 && !done_ && epochs_ >= next_recompute_) {
         recompute_fields();
         next_recompute_ = epochs_ + recompute_epochs_;
     }
@@ -610,8 +612,7 @@ cudaGraph_t Engine::epoch_graph() {
         a.count = static_cast<int32_t>(walkers_);
         a.epoch_mode = 1;
         a.smem_per_walker = static_cast<int32_t>(walker_smem_bytes(view_, smem_fields_, features_));
-        launch_walk(view_, a, walkers_per_block, stream_);  // sets the kernel attributes
-        launch_exchange(view_, stream_);
+        launch_epoch(a);  // sets the kernel attributes
         after_epochs();
         build_graph();
     }
@@ -723,6 +724,7 @@ void Engine::time_epochs(uint64_t epochs, wlg_epoch_timing* out) {
             check_cuda(cudaEventRecord(ev[3 * k + 1], stream_), "record");
             launch_exchange(view_, stream_);
             check_cuda(cudaEventRecord(ev[3 * k + 2], stream_), "record");
+            if (recompute_epochs_ == 1) launch_recompute();
             check_cuda(cudaEventRecord(ev[3 * k + 3], stream_), "record");
             ++ran;
         }
@@ -1229,7 +1231,7 @@ void Engine::save_run(const std::string& path) {
     hd.emin = cfg_.emin;
     hd.emax = cfg_.emax;
     hd.width = cfg_.bin_width;
-    hd.recomputes = recomputes_;
+    hd.recomputes = rep.recomputes;
     hd.next_recompute_in = next_recompute_ > epochs_ ? next_recompute_ - epochs_ : 0;
     const std::string tmp = path + ".tmp";
     {
@@ -1346,7 +1348,6 @@ void Engine::load_run(const std::string& path) {
     check_cuda(cudaStreamSynchronize(stream_), "restore");
     done_ = ctl.done != 0;
     epochs_ = ctl.epoch;
-    recomputes_ = hd.recomputes;
     if (recompute_epochs_) next_recompute_ = epochs_ + hd.next_recompute_in;
     last_checkpoint_ = st[0].attempted;
 }

@@ -286,6 +286,8 @@ class Engine {
     void build_graph();
     void maybe_checkpoint();
     void recompute_fields();
+    void launch_recompute();
+    void launch_epoch(const WalkArgs& a);
     void after_epochs();
     void finish();
     void print_progress(bool final_line);
@@ -310,7 +312,7 @@ class Engine {
         d_rep_spins_, d_ctl_, d_scratch_;
     // mixed precision: FP64 recompute every recompute_epochs_ epochs (0 = never)
     DeviceBuffer d_rfields_, d_renergy_, d_prec_;
-    uint64_t recompute_epochs_ = 0, next_recompute_ = 0, recomputes_ = 0;
+    uint64_t recompute_epochs_ = 0, next_recompute_ = 0;
     EngineView view_{};
 
     std::string checkpoint_path_;

@@ -296,6 +296,35 @@ __global__ void fields_kernel(EngineView v, const int8_t* __restrict__ spins, in
     fields[k * field_stride + i] = sum;
 }
 
+// local_fields of dense couplings for kFieldGroup configurations per block: their spins are
+// staged in shared memory and each J column entry read once serves all of them.  Every field
+// is still summed sequentially over j with the same operations, so the result is the one of
+// fields_kernel.
+constexpr int kFieldGroup = 8;
+__global__ void fields_group_kernel(EngineView v, const int8_t* __restrict__ spins, int64_t spin_stride,
+                                    double* __restrict__ fields, int64_t field_stride, int count) {
+    extern __shared__ int8_t staged[];  // kFieldGroup x n
+    const int k0 = static_cast<int>(blockIdx.y) * kFieldGroup;
+    const int group = min(kFieldGroup, count - k0);
+    for (int q = threadIdx.x; q < group * v.n; q += blockDim.x)
+        staged[q] = spins[(k0 + q / v.n) * spin_stride + q % v.n];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= v.n) return;
+    double sum[kFieldGroup];
+#pragma unroll
+    for (int g = 0; g < kFieldGroup; ++g) sum[g] = 0.0;
+    for (int j = 0; j < v.n; ++j) {
+        const double Jji = v.J64[static_cast<size_t>(j) * v.ld + i];
+#pragma unroll
+        for (int g = 0; g < kFieldGroup; ++g)
+            if (g < group) sum[g] += Jji * static_cast<double>(staged[g * v.n + j]);
+    }
+#pragma unroll
+    for (int g = 0; g < kFieldGroup; ++g)
+        if (g < group) fields[(k0 + g) * field_stride + i] = sum[g];
+}
+
 // total_energy: one thread per configuration, sequential over i.
 __global__ void energy_kernel(int n, const int8_t* __restrict__ spins, int64_t spin_stride,
                               const double* __restrict__ fields, int64_t field_stride, double* __restrict__ out,
@@ -435,9 +464,17 @@ void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream) {
 void compute_fields(const EngineView& v, const int8_t* spins, int64_t spin_stride, double* fields,
                     int64_t field_stride, double* energies, int count, cudaStream_t stream) {
     if (count <= 0) return;
-    const dim3 grid(static_cast<unsigned>((v.n + 127) / 128), static_cast<unsigned>(count));
-    fields_kernel<<<grid, 128, 0, stream>>>(v, spins, spin_stride, fields, field_stride, count);
-    check_cuda(cudaGetLastError(), "fields_kernel");
+    const size_t staged = static_cast<size_t>(kFieldGroup) * static_cast<size_t>(v.n);
+    if (!v.csr && count > 1 && staged <= 48 * 1024) {
+        const dim3 grid(static_cast<unsigned>((v.n + 127) / 128),
+                        static_cast<unsigned>((count + kFieldGroup - 1) / kFieldGroup));
+        fields_group_kernel<<<grid, 128, staged, stream>>>(v, spins, spin_stride, fields, field_stride, count);
+        check_cuda(cudaGetLastError(), "fields_group_kernel");
+    } else {
+        const dim3 grid(static_cast<unsigned>((v.n + 127) / 128), static_cast<unsigned>(count));
+        fields_kernel<<<grid, 128, 0, stream>>>(v, spins, spin_stride, fields, field_stride, count);
+        check_cuda(cudaGetLastError(), "fields_kernel");
+    }
     if (energies) {
         energy_kernel<<<static_cast<unsigned>((count + 127) / 128), 128, 0, stream>>>(
             v.n, spins, spin_stride, fields, field_stride, energies, count);

@@ -13,7 +13,8 @@
 //     window: that resync is deferred to the next interval and counted, so a walker is never
 //     moved out of its window by a correction.
 // The drift maxima, recompute, deferral and bin-change counts accumulate in a
-// PrecisionReport on the device, read by wlg_engine_precision_report.
+// PrecisionReport on the device, read by wlg_engine_precision_report.  A recompute after the
+// epoch that terminated the run changes nothing and is not counted.
 #include "engine.hpp"
 #include "walker_dev.cuh"
 
@@ -36,7 +37,9 @@ __global__ void resync_kernel(EngineView v, const double* __restrict__ rfields, 
                               PrecisionReport* report) {
     const int lane = threadIdx.x & 31;
     const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (w >= v.walkers || v.ctl->error != 0) return;
+    // a run that has terminated is not corrected any more (its results are final)
+    if (w >= v.walkers || v.ctl->error != 0 || v.ctl->done != 0) return;
+    if (w == 0 && lane == 0) atomicAdd(&report->recomputes, 1ULL);
     WalkerState& st = v.ws[w];
     const size_t base = static_cast<size_t>(st.slot) * static_cast<size_t>(v.ld);
     double* f = v.fields + base;
