@@ -127,6 +127,19 @@ def flush_l2(torch, buf):
     buf.add_(1.0)  # 256 MiB written: larger than the 126 MB L2
 
 
+def reduce_over_ranks(dist, device, maxima, sums):
+    """The whole job's figures from every rank's: the maximum over ranks of each time, the sum
+    over ranks of each count (identity with one process).  Every rank calls it at the same point."""
+    if dist is None:
+        return [float(x) for x in maxima], [float(x) for x in sums]
+    import torch
+    t = torch.tensor([float(x) for x in maxima], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(x) for x in sums], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return t.tolist(), c.tolist()
+
+
 def run_ours(args, rank: int, world: int, dist, torch) -> None:
     from replica_exchange_wang_landau_b200 import engine as E
     from replica_exchange_wang_landau_b200._abi import wlg_run_config
@@ -167,15 +180,9 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
         dist.barrier()
     clock = clocks.summary()
     # max over ranks of the device time; total attempts over ranks
-    if dist:
-        tt = torch.tensor([total_ms, walk_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        at = torch.tensor([attempted, accepted], dtype=torch.float64, device="cuda")
-        dist.all_reduce(at, op=dist.ReduceOp.SUM)
-        total_max, walk_max = float(tt[0]), float(tt[1])
-        att_all, acc_all = int(at[0]), int(at[1])
-    else:
-        total_max, walk_max, att_all, acc_all = total_ms, walk_ms, attempted, accepted
+    (total_max, walk_max), (att_all, acc_all) = reduce_over_ranks(dist, "cuda", [total_ms, walk_ms],
+                                                                  [attempted, accepted])
+    att_all, acc_all = int(att_all), int(acc_all)
     value = att_all / (total_max / 1e3)
 
     # host wall-clock throughput of the same path (run_epochs), for context
@@ -226,13 +233,8 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
             e2e_time += dt
             e2e_attempts += totals.attempted
             e2e_accepted += totals.accepted
-    e2e_value = e2e_attempts / e2e_time
-    if dist:
-        et = torch.tensor([e2e_time], dtype=torch.float64, device="cuda")
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
-        ea = torch.tensor([e2e_attempts], dtype=torch.float64, device="cuda")
-        dist.all_reduce(ea, op=dist.ReduceOp.SUM)
-        e2e_value = float(ea[0]) / float(et[0])
+    (e2e_time_max,), (e2e_attempts_all,) = reduce_over_ranks(dist, "cuda", [e2e_time], [e2e_attempts])
+    e2e_value = e2e_attempts_all / e2e_time_max
 
     # roofline of the sweep kernel: algorithmic bytes = one FP64 J row (N x 8 bytes) per
     # accepted flip (fields, spins and the window's log_g/H live in shared memory)
