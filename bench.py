@@ -19,6 +19,7 @@ star fixes one GPU per run; windows are not sharded), timed on the device, max o
 from __future__ import annotations
 
 import argparse
+import copy
 import ctypes as C
 import json
 import os
@@ -192,6 +193,8 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
     eng.run_epochs(epochs * min(args.steps, 5))
     torch.cuda.synchronize()
     graph_rate = (eng.totals()["attempted"] - before) / (time.perf_counter() - g0)
+    active_bins = float(np.mean([st["active_bins"] for st in eng.walker_statistics()]))
+    window_bins = float(np.mean([e - b for b, e in (eng.window(k) for k in range(config.windows))]))
     eng.close()
 
     # e2e through the C-ABI with pinned host buffers: create (H2D geometry) -> run -> fragments (D2H)
@@ -288,6 +291,11 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
                 line["csr_batched"] = csr_batched_line()
             except Exception as exc:
                 line["csr_batched"] = {"error": str(exc)}
+            if cpu:
+                try:
+                    line["time_to_converge"] = time_to_converge(value, cpu["value"], active_bins, window_bins)
+                except Exception as exc:
+                    line["time_to_converge"] = {"error": str(exc)}
             try:
                 line["time_to_accuracy"] = time_to_accuracy()
             except Exception as exc:
@@ -462,6 +470,55 @@ def time_to_accuracy(tolerance: float = 0.05) -> dict:
             "held_out": rows, "plain_attempts_per_walker": pa, "learned_attempts_per_walker": la,
             "plain_seconds": ps, "learned_seconds": ls, "attempts_ratio": la / pa if pa else None,
             "seconds_ratio": ls / ps if ps else None}
+
+
+def c1_config():
+    """The plain CPU-runnable configuration: 2x2x2 open simple cubic (N = 8), +z axes, dense FP64
+    J, grid [-20, 20] in bins of 0.25, 1 window x 2 walkers, flatness 0.8 then 1/t to ln f = 1e-8,
+    seed 1234 (the reference's other defaults)."""
+    from replica_exchange_wang_landau_b200.engine import Geometry, RunConfig, System
+    g = Geometry.simple_cubic(2, 2, 2, 1.0, (0.0, 0.0, 1.0), False)
+    c = RunConfig(emin=-20.0, emax=20.0, bin_width=0.25, windows=1, walkers=2, seed=1234)
+    c.wl.final_factor = 1e-8
+    c.resolve_mcs(g.size())
+    return System(g, 1.0, 0.0), c
+
+
+def time_to_converge(value: float, cpu_value: float, active_bins: float, window_bins: float) -> dict:
+    """Time to ln f <= 1e-8 as an extrapolation: in the 1/t stage ln f = active bins / attempts
+    per walker, so a walker converges after active_bins / 1e-8 attempts; divided by the measured
+    attempts/s per walker.  Walkers run side by side (on the GPU all at once; on the host over
+    its cores), so the time is that of one walker at the per-walker rate.  The dense REWL
+    workload uses this run's rates (active bins now: a lower bound; window bins: an upper one);
+    the N = 8 configuration measures its own rates (2 walkers) on the GPU and on the host."""
+    from replica_exchange_wang_landau_b200.engine import Engine
+    from oracle.oracle import Reference
+    out = {"method": "extrapolation: (active bins / 1e-8) attempts per walker / measured attempts per walker per s"}
+    per_walker_gpu, per_walker_cpu = value / 128, cpu_value / 128
+    out["dense_rewl_512"] = {"attempts_per_walker": [active_bins / 1e-8, window_bins / 1e-8],
+                             "gpu_s": [active_bins / 1e-8 / per_walker_gpu, window_bins / 1e-8 / per_walker_gpu],
+                             "reference_cpu_s": [active_bins / 1e-8 / per_walker_cpu,
+                                                 window_bins / 1e-8 / per_walker_cpu]}
+    system, config = c1_config()
+    with Engine(system, config) as eng:
+        eng.time_run(20)
+        t = eng.time_run(400)
+        gpu_rate = t["attempted"] / config.walkers / (t["total_ms"] / 1e3)
+        active = float(np.mean([st["active_bins"] for st in eng.walker_statistics()]))
+    ref = Reference()
+    used = ref.set_threads(config.walkers)
+    cfg = copy.deepcopy(config)
+    cfg.max_mcs = 2_000_000.0
+    cfg.resolved_spin_count = 0
+    cfg.resolve_mcs(system.size())
+    t0 = time.perf_counter()
+    r = ref.run_rewl(system, cfg)
+    cpu_rate = r.attempted / config.walkers / (time.perf_counter() - t0)
+    need = active / 1e-8
+    out["c1_n8"] = {"active_bins": active, "attempts_per_walker": need, "gpu_attempts_per_walker_per_s": gpu_rate,
+                    "reference_cpu_attempts_per_walker_per_s": cpu_rate, "reference_threads": used,
+                    "gpu_s": need / gpu_rate, "reference_cpu_s": need / cpu_rate}
+    return out
 
 
 def reference_rate(mcs: float, threads: int, seed: int = 1):
