@@ -436,10 +436,10 @@ def _enumerate(system):
     return emin, emax, w, ref
 
 
-def time_to_accuracy(tolerance: float = 0.05) -> dict:
+def time_to_accuracy(tolerance: float = 0.05, held_out: int = 24) -> dict:
     """Learned vs plain: the warm-start network is trained on the GPU on 48 plain-run DOS
-    curves of random dipole clusters (8-12 spins, density 0.3-0.8, random axes); each of 6
-    held-out clusters is then run from the flat start and from the learned start (ln f =
+    curves of random dipole clusters (8-12 spins, density 0.3-0.8, random axes); each of
+    `held_out` other clusters is then run from the flat start and from the learned start (ln f =
     1e-2) until max |d log g| against exact enumeration is <= tolerance."""
     from replica_exchange_wang_landau_b200.warmstart import WarmStartModel, plain_dos_many, run_to_accuracy
     t0 = time.perf_counter()
@@ -453,7 +453,7 @@ def time_to_accuracy(tolerance: float = 0.05) -> dict:
     loss = model.fit(train, steps=4000, learning_rate=3e-3)
     train_s = time.perf_counter() - t0
     rows = []
-    for k in range(101, 107):
+    for k in range(1001, 1001 + held_out):
         s = _cluster(k)
         emin, emax, w, ref = _enumerate(s)
         a = run_to_accuracy(s, emin, emax, w, ref, tolerance, seed=k)
@@ -465,11 +465,15 @@ def time_to_accuracy(tolerance: float = 0.05) -> dict:
     la = sum(r["learned_attempts"] for r in ok)
     ps = sum(r["plain_s"] for r in ok)
     ls = sum(r["learned_s"] for r in ok)
+    ratios = sorted(r["learned_attempts"] / r["plain_attempts"] for r in ok)
     return {"tolerance": tolerance, "criterion": "max |d log g| vs exact enumeration, 1 window x 2 walkers, 1/t",
             "training": {"curves": len(train), "final_loss": loss, "seconds": train_s},
-            "held_out": rows, "plain_attempts_per_walker": pa, "learned_attempts_per_walker": la,
+            "held_out_systems": len(rows), "reached_tolerance": len(ok),
+            "plain_attempts_per_walker": pa, "learned_attempts_per_walker": la,
             "plain_seconds": ps, "learned_seconds": ls, "attempts_ratio": la / pa if pa else None,
-            "seconds_ratio": ls / ps if ps else None}
+            "seconds_ratio": ls / ps if ps else None,
+            "per_system_attempts_ratio": {"min": ratios[0], "median": ratios[len(ratios) // 2], "max": ratios[-1]}
+            if ratios else None}
 
 
 def c1_config():

@@ -77,11 +77,13 @@ def _grid(s: System):
     return math.floor(e.min() / w) * w - w, math.ceil(e.max() / w) * w + w, w
 
 
-def test_learned_warm_start_gain(oracle):
-    """Ablation: the network trained on 48 plain-run DOS curves of random dipole clusters
-    (8-12 spins) starts 6 held-out clusters at ln f = 1e-2; over two seeds each, the learned
-    runs reach max |d log g| <= 0.05 against exact enumeration in fewer total attempts than
-    the same runs from the flat start (measured here: 0.66 of them)."""
+def test_learned_warm_start_ablation(oracle):
+    """Ablation of the learned warm start: the network trained on 48 plain-run DOS curves of
+    random dipole clusters (8-12 spins) starts 8 held-out clusters at ln f = 1e-2, and every run,
+    learned or flat, reaches max |d log g| <= 0.05 against exact enumeration.  At this size the
+    learned start gains nothing measurable: over 24 held-out clusters it took 0.99-1.11 times the
+    attempts of the flat start depending on the start factor (1e-3 to 1e-1), so the test bounds
+    the ratio on both sides instead of asserting a gain."""
     specs = []
     for k in range(1, 49):
         s = _cluster(k)
@@ -90,16 +92,15 @@ def test_learned_warm_start_gain(oracle):
     model = WarmStartModel(hidden=(32, 32), seed=3)
     assert model.fit(train, steps=4000, learning_rate=3e-3) < 0.5
     flat = learned = 0
-    for k in range(101, 107):
+    for k in range(1001, 1009):
         s = _cluster(k)
         emin, emax, w = _grid(s)
         counts = oracle.exact_counts(s, emin, emax, w)
         ref = np.where(counts > 0, np.log(np.maximum(counts, 1).astype(float)), np.nan)
-        for seed in (k, k + 1000):
-            a = run_to_accuracy(s, emin, emax, w, ref, 0.05, seed)
-            b = run_to_accuracy(s, emin, emax, w, ref, 0.05, seed, model=model, factor=1e-2)
-            assert not a["warm"] and b["warm"]
-            assert a["attempts"] is not None and b["attempts"] is not None
-            flat += a["attempts"]
-            learned += b["attempts"]
-    assert learned <= 0.8 * flat, (learned, flat)
+        a = run_to_accuracy(s, emin, emax, w, ref, 0.05, k)
+        b = run_to_accuracy(s, emin, emax, w, ref, 0.05, k, model=model, factor=1e-2)
+        assert not a["warm"] and b["warm"]
+        assert a["attempts"] is not None and b["attempts"] is not None
+        flat += a["attempts"]
+        learned += b["attempts"]
+    assert 0.5 * flat <= learned <= 1.5 * flat, (learned, flat)
