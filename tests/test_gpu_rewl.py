@@ -48,6 +48,11 @@ CASES = {
               dict(emin=-150, emax=150, bin_width=0.5, windows=2, walkers=3, seed=9)),
     "dense100": (lambda: _random_system((5, 5, 4), 14),
                  dict(emin=-150, emax=150, bin_width=1.0, windows=2, walkers=2, seed=17)),
+    # the headline system size (512 sites: eight 64-field chunks per lane) and 216 sites (four)
+    "dense512": (lambda: _random_system((8, 8, 8), 18),
+                 dict(emin=-228.5, emax=228.0, bin_width=0.5, windows=3, walkers=2, seed=19)),
+    "dense216": (lambda: _random_system((6, 6, 6), 20),
+                 dict(emin=-150, emax=150, bin_width=0.75, windows=2, walkers=2, seed=23)),
     "collect": (lambda: _random_system((3, 3, 2), 15),
                 dict(emin=-40, emax=40, bin_width=0.5, windows=3, walkers=2, seed=2,
                      wl=WlParameters(collect_window_statistics=True))),
@@ -98,6 +103,13 @@ RUNS = {
                                    exchange_interval_mcs=1, check_interval_mcs=3),
                               dict(nalivaiko_mod=True, inverse_time_enabled=False, flatness=0.5, minimum_visits=5,
                                    final_factor=1e-3)),
+    "dense512_exchange": (lambda: _random_system((8, 8, 8), 18),
+                          dict(emin=-228.5, emax=228.0, bin_width=0.5, windows=4, walkers=2, seed=29, max_mcs=40,
+                               exchange_interval_mcs=1, check_interval_mcs=4), dict(final_factor=1e-2)),
+    "dense216_frozen": (lambda: _random_system((6, 6, 6), 20),
+                        dict(emin=-150, emax=150, bin_width=0.75, windows=2, walkers=2, seed=31, max_mcs=400,
+                             exchange_interval_mcs=1, check_interval_mcs=2),
+                        dict(flatness=0.2, minimum_visits=2, final_factor=5e-2, inverse_time_enabled=False)),
     "forced": (lambda: _random_system((3, 2, 2), 17),
                dict(emin=-30, emax=30, bin_width=0.25, windows=2, walkers=2, seed=8, max_mcs=80,
                     exchange_interval_mcs=1, force_accept_after_mcs=0.5), dict(final_factor=1e-2)),
