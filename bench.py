@@ -288,6 +288,10 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
             except Exception as exc:  # reported, never fatal to the headline line
                 line["mixed_precision"] = {"error": str(exc)}
             try:
+                line["batched_instances"] = batched_instances_line()
+            except Exception as exc:
+                line["batched_instances"] = {"error": str(exc)}
+            try:
                 line["csr_batched"] = csr_batched_line()
             except Exception as exc:
                 line["csr_batched"] = {"error": str(exc)}
@@ -370,6 +374,52 @@ def mixed_precision_lines(epochs: int = 10) -> dict:
                        "random-sphere axes, dense J; 32 windows x 8 walkers, exchange and FP64 recompute every MCS; "
                        f"grid [{config.emin:g}, {config.emax:g}] in bins of {config.bin_width:g}")
     return out
+
+
+def batched_instances_line(count: int = 256, epochs: int = 32) -> dict:
+    """The batched configuration's scale: `count` dilute random systems (N uniform in 64..1024,
+    random sequential addition in a periodic cube at density 0.3-0.8, minimum separation 0.8,
+    random-sphere axes; seeded), each one window x 2 walkers over about +-4 sigma of its
+    random-configuration energy distribution in 200 power-of-two bins, advanced together by
+    single graph launches (Batch) and, for comparison, one engine after the other; wall-clock
+    attempts/s of both, host synchronisation included."""
+    import math
+    from replica_exchange_wang_landau_b200.engine import Batch, Engine, RunConfig, System
+    from replica_exchange_wang_landau_b200.geometry import random_sequential
+    t0 = time.perf_counter()
+    engines, sizes = [], []
+    try:
+        for k in range(count):
+            rng = np.random.default_rng(50_000 + k)
+            n = int(rng.integers(64, 1025))
+            s = System(random_sequential(n, float(rng.uniform(0.3, 0.8)), 0.8, seed=50_000 + k), 1.0, 0.0)
+            sigma = math.sqrt(0.5 * float(np.sum(s.couplings("fp64") ** 2)))
+            w = 2.0 ** round(math.log2(8.0 * sigma / 200.0))
+            c = RunConfig(emin=-100.0 * w, emax=100.0 * w, bin_width=w, windows=1, walkers=2, seed=k + 1)
+            c.resolve_mcs(n)
+            engines.append(Engine(s, c))
+            sizes.append(n)
+        setup_s = time.perf_counter() - t0
+
+        def attempted() -> int:
+            return sum(e.totals()["attempted"] for e in engines)
+
+        with Batch(engines) as batch:
+            batch.run_epochs(16)  # warm
+            a0, t1 = attempted(), time.perf_counter()
+            batch.run_epochs(epochs)
+            batched = (attempted() - a0) / (time.perf_counter() - t1)
+        a0, t1 = attempted(), time.perf_counter()
+        for e in engines:
+            e.run_epochs(epochs)
+        sequential = (attempted() - a0) / (time.perf_counter() - t1)
+    finally:
+        for e in engines:
+            e.close()
+    return {"value": batched, "unit": UNIT, "systems": count, "walkers": 2 * count,
+            "spins": {"min": min(sizes), "mean": float(np.mean(sizes)), "max": max(sizes)},
+            "sequential_attempts_per_s": sequential, "batched_over_sequential": batched / sequential,
+            "epochs": epochs, "setup_s": setup_s, "timing": "wall clock, host synchronisation included"}
 
 
 def csr_batched_line(epochs: int = 40, pilot_mcs: float = 20.0) -> dict:
@@ -591,6 +641,8 @@ def main() -> None:
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--skip-extras", action="store_true",
                     help="skip the mixed-precision lines and the learned-vs-plain time to accuracy")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="print only the batched-instances line (256 dilute systems, N 64..1024)")
     ap.add_argument("--mixed-only", action="store_true",
                     help="print only the mixed-precision configuration's lines (N = 2458, FP64 / FP32 / BF16)")
     ap.add_argument("--csr-only", action="store_true",
@@ -598,6 +650,9 @@ def main() -> None:
     args = ap.parse_args()
     if args.csr_only:
         print(json.dumps({"csr_batched": csr_batched_line()}))
+        return
+    if args.batched_only:
+        print(json.dumps({"batched_instances": batched_instances_line()}))
         return
     if args.mixed_only:
         print(json.dumps({"mixed_precision": mixed_precision_lines()}))
