@@ -13,7 +13,6 @@ from __future__ import annotations
 import ctypes as C
 import math
 from dataclasses import dataclass, field
-from pathlib import Path
 from typing import Optional, Sequence
 
 import numpy as np

@@ -2,7 +2,6 @@
 engines run one after another."""
 from __future__ import annotations
 
-import numpy as np
 import pytest
 
 from helpers import snapshots_equal

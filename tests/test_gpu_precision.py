@@ -8,7 +8,7 @@ import math
 import numpy as np
 import pytest
 
-from replica_exchange_wang_landau_b200.engine import Engine, Geometry, RunConfig, System, WlParameters, run_rewl
+from replica_exchange_wang_landau_b200.engine import Engine, RunConfig, System, WlParameters, run_rewl
 from replica_exchange_wang_landau_b200.geometry import simple_cubic_random
 
 pytestmark = pytest.mark.gpu
