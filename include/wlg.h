@@ -390,6 +390,11 @@ wlg_status wlg_write_dos_csv(const char* path, double emin, double width, uint64
 wlg_status wlg_write_fragment_csv(const char* path, double emin, double width, uint64_t window_id,
                                   uint64_t window_begin, uint64_t window_end, const double* log_g,
                                   const uint64_t* histogram, const double* standard_error, const uint8_t* valid);
+/* The reference's <prefix>_workers_stat.csv (write_workers_stat_csv, src/io.cpp:430-451), byte
+ * for byte: one row per walker statistic, the MCS columns divided by spin_count (0 is
+ * WLG_ERR_INVALID_ARGUMENT, "Cannot write MCS statistics for zero spins"). */
+wlg_status wlg_write_workers_stat_csv(const char* path, const wlg_walker_statistics* statistics, uint64_t count,
+                                      uint64_t spin_count);
 
 /* ---- the adaptive-window pilot (apps/wl_run.cpp:104-169; src/analysis.cpp:183-420) ------ */
 /* wl::AdaptiveWindowParameters (include/wl/analysis.hpp:28-38). */

@@ -284,6 +284,8 @@ class Reference(_Checker):
                                          P(_u64), P(_dbl), P(C.c_uint8), P(_u64), C.c_char_p, _cp, _sz]),
             "ref_write_fragment_csv": (C.c_int, [C.c_char_p, _dbl, _dbl, _dbl, P(_abi.wlg_fragment_view), _u64, _cp,
                                                  _sz]),
+            "ref_write_workers_stat_csv": (C.c_int, [C.c_char_p, P(_abi.wlg_walker_statistics), _u64, _u64, _cp,
+                                                     _sz]),
             "ref_select_initial": (C.c_int, [_vp, _dbl, _dbl, _dbl, P(_u64), _u64, _u64, _u64, P(C.c_int8),
                                              P(C.c_uint8), P(_u64), P(_u64), _cp, _sz]),
         }
@@ -315,6 +317,11 @@ class Reference(_Checker):
         err = _err()
         _raise(self.lib.ref_write_fragment_csv(str(path).encode(), emin, emax, width, C.byref(view), window_id, err,
                                                len(err)), err)
+
+    def write_workers_stat_csv(self, path, rows, spins: int) -> None:
+        """wl::write_workers_stat_csv on a ctypes array of wlg_walker_statistics."""
+        err = _err()
+        _raise(self.lib.ref_write_workers_stat_csv(str(path).encode(), rows, len(rows), spins, err, len(err)), err)
 
     def couplings(self, system: System) -> np.ndarray:
         n = system.size()

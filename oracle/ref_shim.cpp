@@ -443,6 +443,33 @@ int ref_write_fragment_csv(const char* path, double emin, double emax, double wi
     } catch (const std::exception& e) { put_error(err, errlen, e.what()); return status_of(e); }
 }
 
+// wl::write_workers_stat_csv (src/io.cpp:430-451) on wlg_walker_statistics rows.
+int ref_write_workers_stat_csv(const char* path, const wlg_walker_statistics* s, uint64_t count, uint64_t spins,
+                               char* err, size_t errlen) {
+    try {
+        std::vector<wl::WalkerStatistics> rows(count);
+        for (uint64_t k = 0; k < count; ++k) {
+            auto& r = rows[k];
+            r.walker_id = s[k].walker_id;
+            r.window_id = s[k].window_id;
+            r.mpi_rank = s[k].mpi_rank;
+            r.attempted = s[k].attempted;
+            r.accepted = s[k].accepted;
+            r.forced_accepted = s[k].forced_accepted;
+            r.attempts_since_last_accepted = s[k].attempts_since_last_accepted;
+            r.energy = s[k].energy;
+            r.factor = s[k].factor;
+            r.active_bins = s[k].active_bins;
+            r.minimum_histogram = s[k].minimum_histogram;
+            r.mean_histogram = s[k].mean_histogram;
+            r.min_over_mean = s[k].min_over_mean;
+            r.round_trips = s[k].round_trips;
+        }
+        wl::write_workers_stat_csv(path, rows, spins);
+        return 0;
+    } catch (const std::exception& e) { put_error(err, errlen, e.what()); return status_of(e); }
+}
+
 int ref_select_initial(void* handle, double emin, double emax, double width, const uint64_t* windows, uint64_t count,
                        uint64_t walkers, uint64_t n, int8_t* spins_out, uint8_t* present_out, uint64_t* missing,
                        uint64_t* external, char* err, size_t errlen) {

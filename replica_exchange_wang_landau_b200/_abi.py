@@ -278,6 +278,7 @@ SIGNATURES = {
     "wlg_write_dos_csv": (_i32, [C.c_char_p, _dbl, _dbl, _u64, P(_dbl), P(_u64), P(_dbl), P(C.c_uint8)]),
     "wlg_write_fragment_csv": (_i32, [C.c_char_p, _dbl, _dbl, _u64, _u64, _u64, P(_dbl), P(_u64), P(_dbl),
                                       P(C.c_uint8)]),
+    "wlg_write_workers_stat_csv": (_i32, [C.c_char_p, P(wlg_walker_statistics), _u64, _u64]),
     "wlg_adapt_energy_windows": (_i32, [_dbl, _dbl, _dbl, P(wlg_fragment_view), P(wlg_sampling_view), _u64, _dbl,
                                         P(wlg_adaptive_parameters), P(_u64)]),
     "wlg_select_initial_configurations": (_i32, [_dbl, _dbl, _dbl, P(_u64), _u64, P(_dbl), P(C.c_int8),

@@ -600,6 +600,14 @@ wlg_status wlg_write_fragment_csv(const char* path, double emin, double width, u
     });
 }
 
+wlg_status wlg_write_workers_stat_csv(const char* path, const wlg_walker_statistics* statistics, uint64_t count,
+                                      uint64_t spin_count) {
+    return guarded([&] {
+        if (!path || (count != 0 && !statistics)) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        wlg::write_workers_stat_csv(path, statistics, count, spin_count);
+    });
+}
+
 // ---- the adaptive-window pilot's host steps ------------------------------------------
 
 wlg_status wlg_adapt_energy_windows(double emin, double emax, double width, const wlg_fragment_view* fragments,

@@ -122,6 +122,8 @@ void write_dos_csv(const char* path, double emin, double width, uint64_t bins, c
 void write_fragment_csv(const char* path, double emin, double width, uint64_t window_id, uint64_t begin,
                         uint64_t end, const double* log_g, const uint64_t* histogram, const double* standard_error,
                         const uint8_t* valid);
+void write_workers_stat_csv(const char* path, const wlg_walker_statistics* stats, uint64_t count,
+                            uint64_t spin_count);
 
 // physics.cu
 void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream);

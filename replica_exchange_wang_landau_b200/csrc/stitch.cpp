@@ -192,4 +192,30 @@ void write_fragment_csv(const char* path, double emin, double width, uint64_t wi
             << h[i] << ',' << se[i] << ',' << static_cast<unsigned>(ok[i]) << '\n';
 }
 
+// <prefix>_workers_stat.csv (src/io.cpp:430-451): one row per walker; the MCS columns divide
+// the attempt counts by the spin count, and the acceptance percentage is 0 for a walker that
+// made no attempt.
+void write_workers_stat_csv(const char* path, const wlg_walker_statistics* stats, uint64_t count,
+                            uint64_t spin_count) {
+    if (spin_count == 0) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Cannot write MCS statistics for zero spins");
+    std::ofstream out(path);
+    if (!out) throw WlgError(WLG_ERR_IO, std::string("Cannot write ") + path);
+    out << "mpi_rank,window,walker_id,attempted_flips,attempted_mcs,accepted,forced_accepted,accepted_percent,"
+           "attempts_since_last_accepted,mcs_since_last_accepted,energy,factor,active_bins,min_h,mean_h,"
+           "min_over_mean,round_trips\n"
+        << std::setprecision(17);
+    const double spins = static_cast<double>(spin_count);
+    for (uint64_t k = 0; k < count; ++k) {
+        const wlg_walker_statistics& s = stats[k];
+        const double percent =
+            s.attempted == 0 ? 0.0 : 100.0 * static_cast<double>(s.accepted) / static_cast<double>(s.attempted);
+        out << s.mpi_rank << ',' << s.window_id << ',' << s.walker_id << ',' << s.attempted << ','
+            << static_cast<double>(s.attempted) / spins << ',' << s.accepted << ',' << s.forced_accepted << ','
+            << percent << ',' << s.attempts_since_last_accepted << ','
+            << static_cast<double>(s.attempts_since_last_accepted) / spins << ',' << s.energy << ',' << s.factor
+            << ',' << s.active_bins << ',' << s.minimum_histogram << ',' << s.mean_histogram << ','
+            << s.min_over_mean << ',' << s.round_trips << '\n';
+    }
+}
+
 }  // namespace wlg

@@ -826,6 +826,17 @@ def write_dos_csv(path: str, dos: DensityOfStates) -> None:
                                             _u8ptr(np.ascontiguousarray(dos.valid, np.uint8))))
 
 
+def write_workers_stat_csv(path: str, statistics: Sequence[dict], spin_count: int) -> None:
+    """<prefix>_workers_stat.csv in the reference's format (src/io.cpp:430-451), byte for byte, from
+    walker statistics as RewlResult.walker_statistics and Engine.walker_statistics() hold them;
+    spin_count 0 raises InvalidArgument, as the reference's invalid_argument."""
+    rows = (_abi.wlg_walker_statistics * max(1, len(statistics)))()
+    for k, s in enumerate(statistics):
+        for name, _ in _abi.wlg_walker_statistics._fields_:
+            setattr(rows[k], name, s[name])
+    _check(load_library().wlg_write_workers_stat_csv(str(path).encode(), rows, len(statistics), int(spin_count)))
+
+
 def write_fragment_csv(path: str, fragment: DosFragment, emin: float, width: float, window_id: int) -> None:
     """<prefix>_window_<w>.csv in the reference's format (src/io.cpp:410-421), byte for byte."""
     v, arrays = _fragment_view(fragment)
