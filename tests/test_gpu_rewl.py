@@ -11,7 +11,7 @@ import pytest
 from helpers import config_from, random_axes, results_equal, snapshots_equal, system_from, unhex, same_double
 from replica_exchange_wang_landau_b200.engine import (Engine, EscapedError, Geometry, InitializationError,
                                                       InvalidArgument, LogicError, RunConfig, System, WlParameters,
-                                                      run_rewl)
+                                                      run_rewl, write_workers_stat_csv)
 
 pytestmark = pytest.mark.gpu
 
@@ -166,8 +166,8 @@ def test_rewl_vs_exact_2x2x1(oracle):
     assert results_equal(r, again) == []
 
 
-def test_unlimited_and_blocked_runs():
-    """tests/test_main.cpp:282-362 (serial part)."""
+def test_unlimited_and_blocked_runs(tmp_path):
+    """tests/test_main.cpp:282-362 (serial part), the blocked walker's workers-stat CSV row included."""
     one = System(Geometry.simple_cubic(1, 1, 1, 1.0, (0, 0, 1), False))
     c = RunConfig(emin=-1, emax=1, bin_width=0.5, windows=1, walkers=1)
     c.exchange_interval_attempts, c.max_attempts = 1, 0
@@ -197,6 +197,8 @@ def test_unlimited_and_blocked_runs():
     assert (st["attempted"], st["accepted"], st["attempts_since_last_accepted"]) == (5, 0, 5)
     assert st["factor"] == 1.0 and st["active_bins"] == 1 and st["minimum_histogram"] == 6
     assert st["mean_histogram"] == 6.0 and st["min_over_mean"] == 1.0 and st["energy"] == 1.0
+    write_workers_stat_csv(tmp_path / "ws.csv", r.walker_statistics, two.size())
+    assert (tmp_path / "ws.csv").read_text().split("\n")[1] == "0,0,0,5,2.5,0,0,0,5,2.5,1,1,1,6,6,1,0"
 
 
 def test_forced_acceptance():
