@@ -303,6 +303,14 @@ wlg_status wlg_engine_autotune(wlg_engine* engine, uint64_t trial_epochs, wlg_au
  * replay (>= 1); 0 leaves a value unchanged.  No counterpart in the reference. */
 wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block,
                                  int32_t epochs_per_graph);
+/* Single-window runs of small dense systems (one window, FP64 couplings, at most 32 sites
+ * and 4 walkers, no pilot statistics or Nalivaiko mask) run many epochs per launch in one
+ * CTA; this is the default for such engines.  enabled = 0 selects the per-epoch kernels
+ * instead (same results); for other engines the call changes nothing.  No counterpart in
+ * the reference. */
+wlg_status wlg_engine_set_window_sweep(wlg_engine* engine, int32_t enabled);
+/* 1 when the engine runs its epochs with the single-window kernel, else 0. */
+int32_t wlg_engine_window_sweep(const wlg_engine* engine);
 /* The drift report of a mixed-precision run (all zero for FP64 couplings).  No counterpart
  * in the reference. */
 wlg_status wlg_engine_precision_report(wlg_engine* engine, wlg_precision_report* out);

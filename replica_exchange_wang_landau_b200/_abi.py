@@ -296,6 +296,8 @@ SIGNATURES = {
     "wlg_mlp_gradients": (_i32, [_vp, P(C.c_float), P(C.c_float), _u64, P(C.c_float), P(_dbl)]),
     "wlg_mlp_train": (_i32, [_vp, P(C.c_float), P(C.c_float), _u64, _u64, _dbl, P(_dbl)]),
     "wlg_engine_set_launch": (_i32, [_vp, _i32, _i32]),
+    "wlg_engine_set_window_sweep": (_i32, [_vp, _i32]),
+    "wlg_engine_window_sweep": (_i32, [_vp]),
     "wlg_engine_walkers": (_u64, [_vp]),
     "wlg_engine_bins": (_u64, [_vp]),
     "wlg_engine_spins": (_u64, [_vp]),

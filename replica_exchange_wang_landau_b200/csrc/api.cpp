@@ -385,6 +385,15 @@ wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block, 
     return guarded([&] { engine->impl->set_launch(walkers_per_block, epochs_per_graph); });
 }
 
+wlg_status wlg_engine_set_window_sweep(wlg_engine* engine, int32_t enabled) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] { engine->impl->set_window_sweep(enabled != 0); });
+}
+
+int32_t wlg_engine_window_sweep(const wlg_engine* engine) {
+    return engine && engine->impl && engine->impl->window_sweep() ? 1 : 0;
+}
+
 uint64_t wlg_engine_walkers(const wlg_engine* engine) { return engine && engine->impl ? engine->impl->walkers() : 0; }
 uint64_t wlg_engine_bins(const wlg_engine* engine) { return engine && engine->impl ? engine->impl->bins() : 0; }
 uint64_t wlg_engine_spins(const wlg_engine* engine) { return engine && engine->impl ? engine->impl->spins() : 0; }

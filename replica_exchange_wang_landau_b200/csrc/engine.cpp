@@ -5,6 +5,7 @@
 // of [walk_kernel -> exchange_kernel] pairs captured once in a CUDA graph and replayed; the
 // device keeps the epoch counter and the termination flag, so a replay after termination is
 // a sequence of no-op launches and the host only reads the control block between replays.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -261,6 +262,8 @@ void Engine::initialise_walkers(const wlg_run_config& c) {
     if (sys_.csr && !smem_fields_ && walker_smem_bytes(v, false, features_) > 200 * 1024) v.spins_global = 1;
     if (!sys_.csr && !fields_fit_in_smem(v, features_))
         throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Dense system too large for the shared-memory walker (use a cutoff)");
+    window_sweep_eligible_ = window_sweep_fits(v);
+    window_sweep_ = window_sweep_eligible_;
 
     // Host-prepared walker headers: window, slot, representative targets (ctor lines 104-118).
     std::vector<WalkerState> states(W);
@@ -441,6 +444,14 @@ void Engine::build_graph() {
 }
 
 void Engine::launch_epochs(uint64_t count) {
+    if (window_sweep_) {  // every epoch of the chunk in one launch, no graph
+        while (count > 0) {
+            const uint32_t e = static_cast<uint32_t>(std::min<uint64_t>(count, 1u << 30));
+            launch_sweep_window(view_, e, stream_);
+            count -= e;
+        }
+        return;
+    }
     WalkArgs a{};
     a.first = 0;
     a.count = static_cast<int32_t>(walkers_);
@@ -527,7 +538,11 @@ void Engine::run_epochs(uint64_t max_epochs, uint64_t* epochs_run, int32_t* done
     const uint64_t start = epochs_;
     uint64_t budget = max_epochs;
     while (!done_ && budget > 0) {
-        uint64_t chunk = std::min<uint64_t>(budget, static_cast<uint64_t>(epochs_per_graph));
+        // the single-window kernel runs about a million attempts per walker per launch
+        const uint64_t per_launch =
+            window_sweep_ ? std::clamp<uint64_t>((uint64_t{1} << 20) / std::max<uint64_t>(1, p_.exchange_interval), 1, 4096)
+                          : static_cast<uint64_t>(epochs_per_graph);
+        uint64_t chunk = std::min<uint64_t>(budget, per_launch);
         if (checkpointing_) {
             WalkerState st{};
             check_cuda(cudaMemcpyAsync(&st, d_ws_.ptr, sizeof st, cudaMemcpyDeviceToHost, stream_), "copy state");
@@ -565,6 +580,10 @@ void Engine::recompute_fields() {
 // One epoch of run_rewl on the stream: the sweep, the exchange and, when the recompute
 // interval is one epoch, the FP64 recompute.
 void Engine::launch_epoch(const WalkArgs& a) {
+    if (window_sweep_) {
+        launch_sweep_window(view_, 1, stream_);
+        return;
+    }
     launch_walk(view_, a, walkers_per_block, stream_);
     launch_exchange(view_, stream_);
     if (recompute_epochs_ == 1) launch_recompute();

@@ -183,6 +183,10 @@ void launch_walk(const EngineView& v, const WalkArgs& a, int walkers_per_block, 
 // sweep.cu: the dense sweep; false when the walker does not fit the shared-memory ring.
 bool launch_sweep_dense(const EngineView& v, const WalkArgs& a, cudaStream_t stream);
 bool launch_sweep_csr(const EngineView& v, const WalkArgs& a, int walkers_per_block, cudaStream_t stream);
+// sweep_window.cu: whole epochs of a single-window run of a dense FP64 system of at most 32
+// sites and 4 walkers, without pilot statistics or the Nalivaiko mask, in one launch
+bool window_sweep_fits(const EngineView& v);
+void launch_sweep_window(const EngineView& v, uint32_t epochs, cudaStream_t stream);
 void launch_ell_fill(int n, int width, const int32_t* ptr, const int32_t* col, const double* val64,
                      const float* val32, int32_t* ell_col, double* ell_val64, float* ell_val32, cudaStream_t stream);
 void launch_exchange(const EngineView& v, cudaStream_t stream);
@@ -279,6 +283,11 @@ class Engine {
     // Launch shape (chosen by the autotuner or set explicitly).
     int walkers_per_block = 1;
     int epochs_per_graph = 32;
+    // Single-window runs of small dense systems: whole epochs per launch (sweep_window.cu).
+    // Eligibility is fixed at creation; set_window_sweep(false) selects the per-epoch kernels.
+    bool window_sweep_eligible() const { return window_sweep_eligible_; }
+    bool window_sweep() const { return window_sweep_; }
+    void set_window_sweep(bool on) { window_sweep_ = on && window_sweep_eligible_; }
     int device = 0;  // CUDA device the engine lives on
 
   private:
@@ -295,6 +304,8 @@ class Engine {
     void print_progress(bool final_line);
     std::vector<WalkerState> download_states();
 
+    bool window_sweep_eligible_ = false;
+    bool window_sweep_ = false;
     wlg_run_config cfg_{};
     DeviceParams p_{};
     DeviceSystem sys_;

@@ -583,6 +583,16 @@ class Engine:
     def set_launch(self, walkers_per_block: int = 0, epochs_per_graph: int = 0) -> None:
         _check(self._lib.wlg_engine_set_launch(self._h, int(walkers_per_block), int(epochs_per_graph)))
 
+    @property
+    def window_sweep(self) -> bool:
+        """Whether epochs run in the single-window kernel (one window, small dense FP64 system;
+        many epochs per launch).  Setting False selects the per-epoch kernels (same results)."""
+        return bool(self._lib.wlg_engine_window_sweep(self._h))
+
+    @window_sweep.setter
+    def window_sweep(self, enabled: bool) -> None:
+        _check(self._lib.wlg_engine_set_window_sweep(self._h, int(bool(enabled))))
+
     def totals(self) -> dict:
         t = _abi.wlg_run_totals()
         _check(self._lib.wlg_engine_totals(self._h, C.byref(t)))
