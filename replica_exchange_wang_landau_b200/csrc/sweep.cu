@@ -796,8 +796,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
     auto run = [&](auto it_tag) {
         constexpr bool kIT = decltype(it_tag)::value;
         const bool frozen = stage == kFrozen;
-        double factor_next = factor;
-        if (kIT && active_count != 0) factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + 1);
+        InverseTimeTable itt;  // the 1/t factors of the coming attempts
         for (uint32_t t = 0; t < batch;) {
             if (static_cast<int32_t>(hq + 4 - ready_to) >= 0 && !ensure(hq + 4)) {
                 failed = true;
@@ -880,7 +879,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
 
             // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
             if (kIT && stage == kInverseTime) {
-                factor = factor_next;
+                factor = inverse_time_factor(itt, att0 + t - 1, active_count, factor, lane);
                 if (factor <= P.final_factor) stage = kFrozen;
             }
             const bool move = accepted && nb != cur;
@@ -907,8 +906,6 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
             cur = ncur;
             if (kIT) {
                 lg_cur = stage != kFrozen ? lg_base + factor : lg_base;
-                if (stage == kInverseTime && active_count != 0)
-                    factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + t + 1);
             } else {
                 lg_cur = frozen ? lg_base : lg_base + factor;
             }

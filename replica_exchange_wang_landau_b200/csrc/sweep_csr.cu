@@ -298,8 +298,7 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
     auto run = [&](auto it_tag) {
         constexpr bool kIT = decltype(it_tag)::value;
         const bool frozen = stage == kFrozen;
-        double factor_next = factor;
-        if (kIT && active_count != 0) factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + 1);
+        InverseTimeTable itt;  // the 1/t factors of the coming attempts
         for (uint32_t t = 0; t < batch;) {
             if (i0 < 0) {  // rare: bounded() rejects draw hq; the next draw is the site
                 hq += 1;
@@ -361,7 +360,7 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
 
             // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
             if (kIT && stage == kInverseTime) {
-                factor = factor_next;
+                factor = inverse_time_factor(itt, att0 + t - 1, active_count, factor, lane);
                 if (factor <= P.final_factor) stage = kFrozen;
             }
             const bool move = accepted && nb != cur;
@@ -379,8 +378,6 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
             cur = ncur;
             if (kIT) {
                 lg_cur = stage != kFrozen ? lg_base + factor : lg_base;
-                if (stage == kInverseTime && active_count != 0)
-                    factor_next = static_cast<double>(active_count) / static_cast<double>(att0 + t + 1);
             } else {
                 lg_cur = frozen ? lg_base : lg_base + factor;
             }

@@ -119,6 +119,30 @@ __device__ __forceinline__ void warp_begin_next_iteration(WalkerState& st, uint6
     __syncwarp();
 }
 
+// update_inverse_time_factor (src/wang_landau.cpp:300-315) for consecutive attempts of the 1/t
+// stage: f = active_bins / attempted, the attempted count including the attempt.  An IEEE
+// division is a dependent sequence of about 170 cycles that the warp would otherwise wait for
+// on every attempt; here lane j divides for the j-th attempt of a block of 32 (the same
+// operands, so the same quotient), and an attempt takes its quotient by a shuffle.  A block
+// is recomputed after 32 attempts or when the active-bin count has changed.  With no active
+// bin the factor is left unchanged, as the reference leaves it.
+struct InverseTimeTable {
+    double q = 0.0;        // lane j: active / (first + j + 1)
+    uint64_t active = 0;   // active-bin count of the block
+    uint32_t next = 32;    // the next attempt's lane; 32: no block
+};
+__device__ __forceinline__ double inverse_time_factor(InverseTimeTable& T, uint64_t attempted_before,
+                                                      uint64_t active_bins, double current, int lane) {
+    if (active_bins == 0) return current;
+    if (T.next >= 32 || active_bins != T.active) {
+        T.active = active_bins;
+        T.next = 0;
+        T.q = static_cast<double>(active_bins) /
+              static_cast<double>(attempted_before + static_cast<uint64_t>(lane) + 1);
+    }
+    return __shfl_sync(kFull, T.q, static_cast<int>(T.next++));
+}
+
 // update_round_trip_state (src/wang_landau.cpp:317-330)
 __device__ __forceinline__ void round_trip_update(double energy, double lower, double upper, double margin_fraction,
                                                   int32_t& state, uint64_t& trips) {
