@@ -297,6 +297,7 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_kernel(EngineView v, WalkAr
     bool act_cur = act_s[cur - wb] != 0;
     bool ref_cur = nalivaiko ? ref_s[cur - wb] != 0 : true;
     const uint64_t threshold = v.site_mod.threshold;
+    InverseTimeTable itt;  // the 1/t factors of the coming attempts
 
     for (uint32_t t = 0; t < batch && !failed;) {
         if (q0 < threshold) {  // bounded() rejects this draw; the next one is the site
@@ -357,8 +358,7 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_kernel(EngineView v, WalkAr
         }
         ++t;
         if (stage == kInverseTime) {  // update_inverse_time_factor
-            if (active_count != 0)
-                factor = static_cast<double>(active_count) / static_cast<double>(att0 + t);
+            factor = inverse_time_factor(itt, att0 + t - 1, active_count, factor, lane);
             if (factor <= P.final_factor) stage = kFrozen;
         }
         if (accepted && nb != cur) {  // update_current_bin moves to the new bin
