@@ -839,7 +839,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
             const double Ep = fma(m, h, E);
             const bool in_range = Ep >= g.minimum && Ep <= g.maximum;
             const double qv = kPow2 ? fma(Ep, g.inv_width, neg_min_scaled) : (Ep - g.minimum) / g.width;
-            int nb = in_range ? __double2int_rd(qv) : -1;
+            int nb = in_range ? bin_floor(qv) : -1;
             nb = (nb == gcount && Ep == g.maximum) ? gcount - 1 : nb;
             const bool in_window = nb >= wb && nb < we;
             const double lg_load = lg_s[in_window ? nb - wb : 0];

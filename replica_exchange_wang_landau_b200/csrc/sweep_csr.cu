@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
             const double Ep = fma(m, slot_field(o), E);
             const bool in_range = Ep >= g.minimum && Ep <= g.maximum;
             const double qv = kPow2 ? fma(Ep, g.inv_width, neg_min_scaled) : (Ep - g.minimum) / g.width;
-            int nb = in_range ? __double2int_rd(qv) : -1;
+            int nb = in_range ? bin_floor(qv) : -1;
             nb = (nb == gcount && Ep == g.maximum) ? gcount - 1 : nb;
             const bool in_window = nb >= wb && nb < we;
             const double lg_load = lg_s[in_window ? nb - wb : 0];

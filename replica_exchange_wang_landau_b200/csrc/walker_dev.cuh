@@ -125,7 +125,8 @@ __device__ __forceinline__ void warp_begin_next_iteration(WalkerState& st, uint6
 // on every attempt; here lane j divides for the j-th attempt of a block of 32 (the same
 // operands, so the same quotient), and an attempt takes its quotient by a shuffle.  A block
 // is recomputed after 32 attempts or when the active-bin count has changed.  With no active
-// bin the factor is left unchanged, as the reference leaves it.
+// bin the factor is left unchanged, as the reference leaves it.  (Reading the quotient by a
+// shuffle issued at the start of the attempt was measured slower.)
 struct InverseTimeTable {
     double q = 0.0;        // lane j: active / (first + j + 1)
     uint64_t active = 0;   // active-bin count of the block
@@ -142,6 +143,11 @@ __device__ __forceinline__ double inverse_time_factor(InverseTimeTable& T, uint6
     }
     return __shfl_sync(kFull, T.q, static_cast<int>(T.next++));
 }
+
+// Floor of a bin coordinate 0 <= q < 2^31 (the grid index of an in-range energy): the sum
+// q + 2^52 rounded toward -infinity is 2^52 + floor(q) exactly (the unit in the last place is
+// 1 there), and its low word is floor(q).  One add instead of a double-to-integer conversion.
+__device__ __forceinline__ int bin_floor(double q) { return __double2loint(__dadd_rd(q, 0x1.0p52)); }
 
 // update_round_trip_state (src/wang_landau.cpp:317-330)
 __device__ __forceinline__ void round_trip_update(double energy, double lower, double upper, double margin_fraction,
