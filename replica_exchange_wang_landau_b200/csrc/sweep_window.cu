@@ -251,6 +251,10 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                 constexpr bool kIT = decltype(it_tag)::value;
                 const bool frozen = stage == kFrozen;
                 InverseTimeTable itt;  // the 1/t factors of the coming attempts
+                // 1/t stage: an attempt's factor and freeze are applied to log g of its bin at the point
+                // where the next attempt first reads log g, so the factor's shuffle is not waited for
+                double lg_base_p = 0.0, f_p = 0.0;
+                bool pend = false;
                 for (uint32_t t = 0; t < batch;) {
                     if (static_cast<int32_t>(hq + 4 - avail) >= 0 && !ensure(hq + 4)) {
                         failed = true;
@@ -283,6 +287,13 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                     nb = (nb == gcount && Ep == g.maximum) ? gcount - 1 : nb;
                     const bool in_window = nb >= wb && nb < we;
                     const double lg_load = lg_s[in_window ? nb - wb : 0];
+                    if (kIT) {  // the previous attempt's factor (update_inverse_time_factor) and log g update
+                        const bool frz = pend && f_p <= P.final_factor;
+                        stage = frz ? kFrozen : stage;
+                        factor = pend ? f_p : factor;
+                        lg_cur = pend ? (frz ? lg_base_p : lg_base_p + f_p) : lg_cur;
+                        pend = false;
+                    }
                     const double lg_new = nb == cur ? lg_cur : lg_load;
                     const double log_ratio = lg_cur - lg_new;
                     const bool det = log_ratio >= 0.0;
@@ -303,9 +314,9 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                     ++t;
 
                     // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
-                    if (kIT && stage == kInverseTime) {
-                        factor = inverse_time_factor(itt, att0 + t - 1, active_count, factor, lane);
-                        if (factor <= P.final_factor) stage = kFrozen;
+                    if (kIT && stage == kInverseTime) {  // resolved at the next read of log g
+                        f_p = inverse_time_factor(itt, att0 + t - 1, active_count, factor, lane);
+                        pend = true;
                     }
                     const bool move = accepted && nb != cur;
                     const int ncur = move ? nb : cur;
@@ -321,7 +332,8 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                     }
                     cur = ncur;
                     if (kIT) {
-                        lg_cur = stage != kFrozen ? lg_base + factor : lg_base;
+                        lg_base_p = lg_base;
+                        lg_cur = lg_base;  // plus the factor once it is resolved (pend)
                     } else {
                         lg_cur = frozen ? lg_base : lg_base + factor;
                     }
@@ -333,6 +345,12 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                     c1 = need_u ? r3 : c2;
                     c2 = need_u ? r4 : r3;
                     lnu = need_u ? l3 : l2;
+                }
+                if (kIT && pend) {  // the last attempt's factor
+                    const bool frz = f_p <= P.final_factor;
+                    stage = frz ? kFrozen : stage;
+                    factor = f_p;
+                    lg_cur = frz ? lg_base_p : lg_base_p + f_p;
                 }
             };
             if (stage == kInverseTime)
