@@ -97,61 +97,43 @@ template <> struct CouplingType<WLG_PRECISION_BF16> { using T = __nv_bfloat16; }
 
 // fields[j] += m * row[j] (add_flip_delta, src/physics.cpp:190-195) from a row in shared
 // memory; m * row[j] is exact (m = +-2, times the BF16 row scale), so fma rounds once as
-// the reference's multiply-then-add does.  FP64 rows update the fields in groups of eight
-// double2 per lane, all of a group's loads issued before its stores, since a shared-memory
-// load issued behind pending stores of the same warp waits for them (measured: 138 -> 189 M
-// attempts/s at N = 2458; the same grouping made the FP32 and BF16 forms slightly slower).
+// the reference's multiply-then-add does.  The fields are updated in groups of eight double2
+// per lane (lane-contiguous, so every access is conflict-free), all of a group's loads issued
+// before its stores, since a shared-memory load issued behind pending stores of the same warp
+// waits for them (FP64, N = 2458: 138 -> 189 M attempts/s).  FP32 and BF16 rows are read as
+// the pair of couplings of each double2 of fields (float2 / one 32-bit word) and widened
+// exactly to double.
 template <int kPrec>
 __device__ __forceinline__ void row_update(const void* row_smem, int ld, double m, double* f, int lane) {
     double2* f2 = reinterpret_cast<double2*>(f);
-    if constexpr (kPrec == WLG_PRECISION_FP64) {
-        constexpr int kGroup = 8;  // double2 per lane per group (16 measured slower)
-        const double2* r = reinterpret_cast<const double2*>(row_smem);
-        const int n2 = ld >> 1;
-        for (int base = 0; base < n2; base += 32 * kGroup) {
-            double2 a[kGroup], h[kGroup];
+    constexpr int kGroup = 8;  // double2 per lane per group (16 measured slower for FP64)
+    const int n2 = ld >> 1;
+    for (int base = 0; base < n2; base += 32 * kGroup) {
+        double2 a[kGroup], h[kGroup];
 #pragma unroll
-            for (int q = 0; q < kGroup; ++q) {
-                const int k = base + lane + 32 * q;
-                if (k < n2) {
-                    a[q] = r[k];
-                    h[q] = f2[k];
+        for (int q = 0; q < kGroup; ++q) {
+            const int k = base + lane + 32 * q;
+            if (k < n2) {
+                if constexpr (kPrec == WLG_PRECISION_FP64) {
+                    a[q] = reinterpret_cast<const double2*>(row_smem)[k];
+                } else if constexpr (kPrec == WLG_PRECISION_FP32) {
+                    const float2 p = reinterpret_cast<const float2*>(row_smem)[k];
+                    a[q] = make_double2(static_cast<double>(p.x), static_cast<double>(p.y));
+                } else {  // BF16 pair: element 2k in the low half of the word, 2k+1 in the high half
+                    const uint32_t w = reinterpret_cast<const uint32_t*>(row_smem)[k];
+                    a[q] = make_double2(static_cast<double>(__uint_as_float(w << 16)),
+                                        static_cast<double>(__uint_as_float(w & 0xffff0000u)));
                 }
-            }
-#pragma unroll
-            for (int q = 0; q < kGroup; ++q) {
-                const int k = base + lane + 32 * q;
-                if (k < n2) {
-                    h[q].x = fma(m, a[q].x, h[q].x);
-                    h[q].y = fma(m, a[q].y, h[q].y);
-                    f2[k] = h[q];
-                }
+                h[q] = f2[k];
             }
         }
-    } else if constexpr (kPrec == WLG_PRECISION_FP32) {
-        const float4* r = reinterpret_cast<const float4*>(row_smem);
-#pragma unroll 2
-        for (int k = lane; k < (ld >> 2); k += 32) {
-            const float4 a = r[k];
-            double2 h0 = f2[2 * k], h1 = f2[2 * k + 1];
-            h0.x = fma(m, static_cast<double>(a.x), h0.x);
-            h0.y = fma(m, static_cast<double>(a.y), h0.y);
-            h1.x = fma(m, static_cast<double>(a.z), h1.x);
-            h1.y = fma(m, static_cast<double>(a.w), h1.y);
-            f2[2 * k] = h0;
-            f2[2 * k + 1] = h1;
-        }
-    } else {
-        const uint4* r = reinterpret_cast<const uint4*>(row_smem);
-        for (int k = lane; k < (ld >> 3); k += 32) {
-            const uint4 raw = r[k];
-            const uint32_t words[4] = {raw.x, raw.y, raw.z, raw.w};
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                double2 h = f2[4 * k + q];
-                h.x = fma(m, static_cast<double>(__uint_as_float(words[q] << 16)), h.x);
-                h.y = fma(m, static_cast<double>(__uint_as_float(words[q] & 0xffff0000u)), h.y);
-                f2[4 * k + q] = h;
+        for (int q = 0; q < kGroup; ++q) {
+            const int k = base + lane + 32 * q;
+            if (k < n2) {
+                h[q].x = fma(m, a[q].x, h[q].x);
+                h[q].y = fma(m, a[q].y, h[q].y);
+                f2[k] = h[q];
             }
         }
     }
