@@ -204,10 +204,10 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
     from replica_exchange_wang_landau_b200.engine import Geometry, System
     pinned_system = System(Geometry(pos.numpy(), axes.numpy(), system.geometry.box, True), 1.0, 0.0)
     bins = config.bins()
-    out_lg = torch.empty(bins, dtype=torch.float64).pin_memory()
-    out_h = torch.empty(bins, dtype=torch.int64).pin_memory()
-    out_se = torch.empty(bins, dtype=torch.float64).pin_memory()
-    out_v = torch.empty(bins, dtype=torch.uint8).pin_memory()
+    out_lg = torch.empty(config.windows * bins, dtype=torch.float64).pin_memory()
+    out_h = torch.empty(config.windows * bins, dtype=torch.int64).pin_memory()
+    out_se = torch.empty(config.windows * bins, dtype=torch.float64).pin_memory()
+    out_v = torch.empty(config.windows * bins, dtype=torch.uint8).pin_memory()
     p_lg = C.cast(out_lg.data_ptr(), C.POINTER(C.c_double))
     p_h = C.cast(out_h.data_ptr(), C.POINTER(C.c_uint64))
     p_se = C.cast(out_se.data_ptr(), C.POINTER(C.c_double))
@@ -226,8 +226,7 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
         E._check(lib.wlg_engine_create(C.byref(sys_s), C.byref(cfg_s), C.byref(handle)))
         ran, done = C.c_uint64(0), C.c_int32(0)
         E._check(lib.wlg_engine_run_epochs(handle, epochs, C.byref(ran), C.byref(done)))
-        for w in range(config.windows):
-            E._check(lib.wlg_engine_fragment(handle, w, 0, p_lg, p_h, p_se, p_v))
+        E._check(lib.wlg_engine_fragments(handle, 0, p_lg, p_h, p_se, p_v))  # every window's fragment
         totals = E._abi.wlg_run_totals()
         E._check(lib.wlg_engine_totals(handle, C.byref(totals)))
         lib.wlg_engine_destroy(handle)
@@ -263,8 +262,8 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
                        "l2": "flushed between timed steps (256 MiB write); J (2 MB) is L2-resident within a step",
                        "parallelism": f"{world} independent replica(s), one per GPU"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "steps": e2e_steps, "path": "wlg_engine_create -> wlg_engine_run_epochs -> wlg_engine_fragment "
-                                                "x16 -> wlg_engine_destroy, pinned host buffers",
+                    "steps": e2e_steps, "path": "wlg_engine_create -> wlg_engine_run_epochs -> wlg_engine_fragments "
+                                                "(all 16 windows) -> wlg_engine_destroy, pinned host buffers",
                     "acceptance": e2e_accepted / max(1, e2e_attempts),
                     "note": "each step is a fresh engine's first epochs; acceptance, and with it the cost of an "
                             "attempt, differs from the long-running engine of value"},

@@ -331,6 +331,11 @@ wlg_status wlg_engine_window(const wlg_engine* engine, uint64_t w, uint64_t* beg
 wlg_status wlg_engine_fragment(wlg_engine* engine, uint64_t w, int32_t allow_empty,
                                double* log_g, uint64_t* histogram, double* standard_error,
                                uint8_t* valid);
+/* Every window's fragment at once (one kernel launch and one copy per array): arrays hold
+ * windows x bins entries, window-major, each window's as wlg_engine_fragment gives it; the
+ * first window without a common active bin fails the call unless allow_empty. */
+wlg_status wlg_engine_fragments(wlg_engine* engine, int32_t allow_empty, double* log_g,
+                                uint64_t* histogram, double* standard_error, uint8_t* valid);
 /* summarize_sampling_impl (src/parallel.cpp:64-78). */
 wlg_status wlg_engine_sampling_statistics(wlg_engine* engine, uint64_t w,
                                           double* squared_energy_displacement,

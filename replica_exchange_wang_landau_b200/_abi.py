@@ -303,6 +303,7 @@ SIGNATURES = {
     "wlg_engine_spins": (_u64, [_vp]),
     "wlg_engine_window": (_i32, [_vp, _u64, P(_u64), P(_u64)]),
     "wlg_engine_fragment": (_i32, [_vp, _u64, _i32, P(_dbl), P(_u64), P(_dbl), P(C.c_uint8)]),
+    "wlg_engine_fragments": (_i32, [_vp, _i32, P(_dbl), P(_u64), P(_dbl), P(C.c_uint8)]),
     "wlg_engine_sampling_statistics": (_i32, [_vp, _u64, P(_dbl), P(_u64), P(_u64), P(_u64)]),
     "wlg_engine_walker_statistics": (_i32, [_vp, P(wlg_walker_statistics), _u64]),
     "wlg_engine_representatives": (_i32, [_vp, P(_dbl), P(C.c_int8), _u64, P(_u64)]),

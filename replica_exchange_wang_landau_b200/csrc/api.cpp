@@ -409,6 +409,16 @@ wlg_status wlg_engine_fragment(wlg_engine* engine, uint64_t w, int32_t allow_emp
     return guarded([&] { engine->impl->fragment(w, allow_empty, log_g, histogram, standard_error, valid); });
 }
 
+wlg_status wlg_engine_fragments(wlg_engine* engine, int32_t allow_empty, double* log_g, uint64_t* histogram,
+                                double* standard_error, uint8_t* valid) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] {
+        if (!log_g || !histogram || !standard_error || !valid)
+            throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null output");
+        engine->impl->fragments(allow_empty, log_g, histogram, standard_error, valid);
+    });
+}
+
 wlg_status wlg_engine_sampling_statistics(wlg_engine* engine, uint64_t w, double* squared_energy_displacement,
                                           uint64_t* displacement_samples, uint64_t* round_trips, uint64_t* walkers) {
     WLG_ENGINE_GUARD(engine)

@@ -864,7 +864,7 @@ void Engine::fragment(uint64_t w, int allow_empty, double* log_g, uint64_t* hist
     double* d_se = reinterpret_cast<double*>(base + 16 * B);
     uint8_t* d_v = reinterpret_cast<uint8_t*>(base + 24 * B);
     int* d_status = reinterpret_cast<int*>(base + ((25 * B + 15) / 16) * 16);
-    launch_summarize(view_, static_cast<int>(w), allow_empty, d_lg, d_h, d_se, d_v, d_status, stream_);
+    launch_summarize(view_, static_cast<int>(w), 1, allow_empty, d_lg, d_h, d_se, d_v, d_status, stream_);
     int status = 0;
     check_cuda(cudaMemcpyAsync(log_g, d_lg, B * 8, cudaMemcpyDeviceToHost, stream_), "copy");
     check_cuda(cudaMemcpyAsync(hist, d_h, B * 8, cudaMemcpyDeviceToHost, stream_), "copy");
@@ -873,6 +873,28 @@ void Engine::fragment(uint64_t w, int allow_empty, double* log_g, uint64_t* hist
     check_cuda(cudaMemcpyAsync(&status, d_status, sizeof status, cudaMemcpyDeviceToHost, stream_), "copy");
     check_cuda(cudaStreamSynchronize(stream_), "summarize");
     if (status) throw WlgError(WLG_ERR_RUNTIME, "Walkers in an energy window have no common active bin");
+}
+
+void Engine::fragments(int allow_empty, double* log_g, uint64_t* hist, double* sem, uint8_t* valid) {
+    const size_t WB = windows_ * bins_;
+    const size_t status_at = ((25 * WB + 15) / 16) * 16;
+    if (!d_frag_.ptr) d_frag_.allocate(status_at + 4 * windows_);
+    char* base = d_frag_.get<char>();
+    double* d_lg = reinterpret_cast<double*>(base);
+    uint64_t* d_h = reinterpret_cast<uint64_t*>(base + 8 * WB);
+    double* d_se = reinterpret_cast<double*>(base + 16 * WB);
+    uint8_t* d_v = reinterpret_cast<uint8_t*>(base + 24 * WB);
+    int* d_status = reinterpret_cast<int*>(base + status_at);
+    launch_summarize(view_, 0, static_cast<int>(windows_), allow_empty, d_lg, d_h, d_se, d_v, d_status, stream_);
+    std::vector<int> status(windows_, 0);
+    check_cuda(cudaMemcpyAsync(log_g, d_lg, WB * 8, cudaMemcpyDeviceToHost, stream_), "copy");
+    check_cuda(cudaMemcpyAsync(hist, d_h, WB * 8, cudaMemcpyDeviceToHost, stream_), "copy");
+    check_cuda(cudaMemcpyAsync(sem, d_se, WB * 8, cudaMemcpyDeviceToHost, stream_), "copy");
+    check_cuda(cudaMemcpyAsync(valid, d_v, WB, cudaMemcpyDeviceToHost, stream_), "copy");
+    check_cuda(cudaMemcpyAsync(status.data(), d_status, 4 * windows_, cudaMemcpyDeviceToHost, stream_), "copy");
+    check_cuda(cudaStreamSynchronize(stream_), "summarize");
+    for (int st : status)
+        if (st) throw WlgError(WLG_ERR_RUNTIME, "Walkers in an energy window have no common active bin");
 }
 
 void Engine::sampling(uint64_t w, double* sq, uint64_t* samples, uint64_t* round_trips, uint64_t* walkers) {

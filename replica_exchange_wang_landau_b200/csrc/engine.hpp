@@ -194,7 +194,8 @@ void launch_exchange(const EngineView& v, cudaStream_t stream);
 void launch_resync(const EngineView& v, const double* rfields, const double* renergy, PrecisionReport* report,
                    cudaStream_t stream);
 void launch_flush_pending(const EngineView& v, cudaStream_t stream);
-void launch_summarize(const EngineView& v, int window, int allow_empty, double* log_g, uint64_t* hist,
+// summarize_impl for windows [window, window + windows): outputs window-major, bins each
+void launch_summarize(const EngineView& v, int window, int windows, int allow_empty, double* log_g, uint64_t* hist,
                       double* sem, uint8_t* valid, int* status, cudaStream_t stream);
 void launch_sampling(const EngineView& v, int window, double* sq, uint64_t* samples, uint64_t* trips,
                      cudaStream_t stream);
@@ -256,6 +257,8 @@ class Engine {
     uint64_t spins() const { return sys_.n; }
     void window(uint64_t w, uint64_t* begin, uint64_t* end) const;
     void fragment(uint64_t w, int allow_empty, double* log_g, uint64_t* hist, double* sem, uint8_t* valid);
+    // every window's fragment in one launch and one copy (arrays windows x bins, window-major)
+    void fragments(int allow_empty, double* log_g, uint64_t* hist, double* sem, uint8_t* valid);
     void sampling(uint64_t w, double* sq, uint64_t* samples, uint64_t* round_trips, uint64_t* walkers);
     void walker_statistics(wlg_walker_statistics* out, uint64_t capacity);
     void representatives(double* energies, int8_t* spins, uint64_t capacity, uint64_t* count);
@@ -322,7 +325,7 @@ class Engine {
 
     DeviceBuffer d_win_begin_, d_win_end_, d_ws_, d_log_g_, d_hist_, d_active_, d_refine_, d_sqdisp_,
         d_dsamples_, d_spins_, d_fields_, d_rep_energy_, d_rep_dist_, d_rep_target_, d_rep_present_,
-        d_rep_spins_, d_ctl_, d_scratch_;
+        d_rep_spins_, d_ctl_, d_scratch_, d_frag_;
     // mixed precision: FP64 recompute every recompute_epochs_ epochs (0 = never)
     DeviceBuffer d_rfields_, d_renergy_, d_prec_;
     uint64_t recompute_epochs_ = 0, next_recompute_ = 0;

@@ -123,11 +123,19 @@ __global__ void flush_pending_kernel(EngineView v) {
 }
 
 // summarize_impl for one window; status 1 = "no common active bin".
-__global__ void summarize_kernel(EngineView v, int window, int allow_empty, double* log_g, uint64_t* hist,
+// One CTA per window: window0 + blockIdx.x, whose outputs (bins entries each) and status are
+// at offset blockIdx.x.
+__global__ void summarize_kernel(EngineView v, int window0, int allow_empty, double* log_g, uint64_t* hist,
                                  double* sem, uint8_t* valid, int* status) {
+    const int window = window0 + static_cast<int>(blockIdx.x);
     const int wb = v.win_begin[window], we = v.win_end[window];
     const int first = window * v.walkers_per_window, count = v.walkers_per_window;
     const size_t bins = static_cast<size_t>(v.grid.count);
+    log_g += blockIdx.x * bins;
+    hist += blockIdx.x * bins;
+    sem += blockIdx.x * bins;
+    valid += blockIdx.x * bins;
+    status += blockIdx.x;
     __shared__ int s_ref;
     if (threadIdx.x == 0) s_ref = we;
     for (size_t i = threadIdx.x; i < bins; i += blockDim.x) {
@@ -319,9 +327,10 @@ void launch_flush_pending(const EngineView& v, cudaStream_t stream) {
     check_cuda(cudaGetLastError(), "flush_pending_kernel");
 }
 
-void launch_summarize(const EngineView& v, int window, int allow_empty, double* log_g, uint64_t* hist, double* sem,
-                      uint8_t* valid, int* status, cudaStream_t stream) {
-    summarize_kernel<<<1, 256, 0, stream>>>(v, window, allow_empty, log_g, hist, sem, valid, status);
+void launch_summarize(const EngineView& v, int window, int windows, int allow_empty, double* log_g, uint64_t* hist,
+                      double* sem, uint8_t* valid, int* status, cudaStream_t stream) {
+    summarize_kernel<<<static_cast<unsigned>(windows), 256, 0, stream>>>(v, window, allow_empty, log_g, hist, sem, valid,
+                                                                         status);
     check_cuda(cudaGetLastError(), "summarize_kernel");
 }
 

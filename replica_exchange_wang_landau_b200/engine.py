@@ -609,6 +609,14 @@ class Engine:
         _check(self._lib.wlg_engine_fragment(self._h, w, int(allow_empty), _dptr(lg), _u64ptr(h), _dptr(se), _u8ptr(v)))
         return DosFragment(self.window(w), lg, h, se, v)
 
+    def fragments(self, allow_empty: bool = False) -> list:
+        """Every window's DosFragment from one launch (wlg_engine_fragments)."""
+        W, B = int(self.config.windows), self.bins
+        lg, h, se, v = np.zeros(W * B), np.zeros(W * B, np.uint64), np.zeros(W * B), np.zeros(W * B, np.uint8)
+        _check(self._lib.wlg_engine_fragments(self._h, int(allow_empty), _dptr(lg), _u64ptr(h), _dptr(se), _u8ptr(v)))
+        return [DosFragment(self.window(w), lg[w * B:(w + 1) * B].copy(), h[w * B:(w + 1) * B].copy(),
+                            se[w * B:(w + 1) * B].copy(), v[w * B:(w + 1) * B].copy()) for w in range(W)]
+
     def sampling_statistics(self, w: int) -> WindowSamplingStatistics:
         B = self.bins
         sq, ds = np.zeros(B), np.zeros(B, np.uint64)
@@ -635,7 +643,7 @@ class Engine:
         """RewlResult as run_rewl assembles it after the loop (src/parallel.cpp:536-580)."""
         t = self.totals()
         collect = self.config.wl.collect_window_statistics
-        fragments = [self.fragment(w, allow_empty=collect) for w in range(int(self.config.windows))]
+        fragments = self.fragments(allow_empty=collect)
         sampling = [self.sampling_statistics(w) for w in range(int(self.config.windows))] if collect else []
         reps = self.representatives() if collect else []
         return RewlResult(fragments, self.walker_statistics(), sampling, reps, t["attempted"], t["accepted"],

@@ -10,8 +10,8 @@ import pytest
 
 from helpers import config_from, random_axes, results_equal, snapshots_equal, system_from, unhex, same_double
 from replica_exchange_wang_landau_b200.engine import (Engine, EscapedError, Geometry, InitializationError,
-                                                      InvalidArgument, LogicError, RunConfig, System, WlParameters,
-                                                      run_rewl, write_workers_stat_csv)
+                                                      InvalidArgument, LogicError, RunConfig, System, WlgError,
+                                                      WlParameters, run_rewl, write_workers_stat_csv)
 
 pytestmark = pytest.mark.gpu
 
@@ -430,3 +430,31 @@ def test_converged_run_matches_reference(reference):
     want = reference.run_rewl(s, c)
     assert got.converged and want.converged
     assert results_equal(got, want) == []
+
+
+def test_fragments_all_windows_equal_per_window():
+    """wlg_engine_fragments (one launch for every window) gives each window's fragment exactly
+    as wlg_engine_fragment does, and fails like it on a window without a common active bin."""
+    s = _random_system((3, 3, 3), 11)
+    c = RunConfig(emin=-60, emax=60, bin_width=0.5, windows=3, walkers=2, seed=21, max_mcs=60,
+                  exchange_interval_mcs=1, check_interval_mcs=10)
+    c.wl.final_factor = 1e-2
+    c.resolve_mcs(s.size())
+    with Engine(s, c) as e:
+        e.run()
+        together = e.fragments()
+        for w in range(c.windows):
+            alone = e.fragment(w)
+            assert together[w].window == alone.window
+            for a, b in ((together[w].log_g, alone.log_g), (together[w].standard_error, alone.standard_error)):
+                assert np.array_equal(np.asarray(a).view(np.uint64), np.asarray(b).view(np.uint64))
+            assert np.array_equal(together[w].histogram, alone.histogram)
+            assert np.array_equal(together[w].valid, alone.valid)
+    fresh = RunConfig(emin=-60, emax=60, bin_width=0.5, windows=3, walkers=2, seed=21)
+    fresh.resolve_mcs(s.size())
+    with Engine(s, fresh) as e:  # no attempt yet: the walkers' visited bins differ
+        e.run_attempts(0, 5)
+        with pytest.raises(WlgError, match="no common active bin"):
+            e.fragments()
+        empty = e.fragments(allow_empty=True)
+        assert len(empty) == 3
