@@ -476,6 +476,12 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_kernel(EngineView v, WalkAr
 //   return) that is folded into H at the end of the batch.  In the Wang-Landau stage the
 //   count of active bins is not read during the batch, so it is updated once, from the active
 //   mask, at the end; in the 1/t stage it is maintained per attempt.
+// * In the 1/t stage the factor active / attempted comes from a table of 32 quotients (one
+//   division per 32 attempts, InverseTimeTable), and an attempt's factor and freeze test are
+//   applied to log g of its bin where the next attempt first reads log g, so neither the
+//   division nor the shuffle that reads the quotient sits on the attempt's chain.
+// * The bin index of an in-range energy is the low word of (q + 2^52) added with rounding
+//   toward -infinity (bin_floor), one add instead of a double-to-integer conversion.
 // * At the end of the batch the walker publishes a stop flag; the producer waits for every
 //   copy it started, and the generator is stepped back over the draws the walker did not
 //   consume, so the stored RNG state is the reference's.  All waits are bounded: on timeout
