@@ -296,45 +296,103 @@ __global__ void fields_kernel(EngineView v, const int8_t* __restrict__ spins, in
     fields[k * field_stride + i] = sum;
 }
 
-// local_fields of dense couplings for kFieldGroup configurations per block: their spins are
-// staged in shared memory and each J column entry read once serves all of them.  Every field
-// is still summed sequentially over j with the same operations, so the result is the one of
-// fields_kernel.
-constexpr int kFieldGroup = 8;
-__global__ void fields_group_kernel(EngineView v, const int8_t* __restrict__ spins, int64_t spin_stride,
-                                    double* __restrict__ fields, int64_t field_stride, int count) {
-    extern __shared__ int8_t staged[];  // kFieldGroup x n
+// local_fields of dense couplings for kFieldGroup configurations per block.  Each thread owns
+// one site i and keeps kFieldGroup sums; the J column entries J[j][i] are read kFieldPrefetch
+// rows ahead into registers, and the configurations' spins are staged as doubles (+-1.0) in
+// shared memory, kFieldTile rows at a time, so that a term is one shared-memory broadcast, one
+// multiply and one add.  Every field is still summed sequentially over j with the reference's
+// operations (sum += J(i, j) * s_j, no contraction), so the result is the one of fields_kernel.
+constexpr int kFieldGroup = 16;
+constexpr int kFieldTile = 256;     // rows j staged per pass (kFieldGroup x kFieldTile doubles = 32 KB)
+constexpr int kFieldPrefetch = 8;   // rows of J in flight per thread
+constexpr int kFieldThreads = 128;
+__global__ void __launch_bounds__(kFieldThreads) fields_group_kernel(EngineView v, const int8_t* __restrict__ spins,
+                                                                      int64_t spin_stride, double* __restrict__ fields,
+                                                                      int64_t field_stride, int count) {
+    __shared__ __align__(16) double sigma[kFieldTile][kFieldGroup];  // row j: the group's spins, contiguous
+    const int n = v.n;
     const int k0 = static_cast<int>(blockIdx.y) * kFieldGroup;
     const int group = min(kFieldGroup, count - k0);
-    for (int q = threadIdx.x; q < group * v.n; q += blockDim.x)
-        staged[q] = spins[(k0 + q / v.n) * spin_stride + q % v.n];
-    __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= v.n) return;
+    const int i = static_cast<int>(blockIdx.x) * kFieldThreads + static_cast<int>(threadIdx.x);
+    const bool site = i < n;
+    const double* __restrict__ col = v.J64 + (site ? i : 0);  // J[j][i] at col[j * ld]
+    const size_t ld = static_cast<size_t>(v.ld);
     double sum[kFieldGroup];
 #pragma unroll
     for (int g = 0; g < kFieldGroup; ++g) sum[g] = 0.0;
-    for (int j = 0; j < v.n; ++j) {
-        const double Jji = v.J64[static_cast<size_t>(j) * v.ld + i];
+    double jv[kFieldPrefetch];
 #pragma unroll
-        for (int g = 0; g < kFieldGroup; ++g)
-            if (g < group) sum[g] += Jji * static_cast<double>(staged[g * v.n + j]);
+    for (int u = 0; u < kFieldPrefetch; ++u) jv[u] = u < n ? col[static_cast<size_t>(u) * ld] : 0.0;
+    for (int t0 = 0; t0 < n; t0 += kFieldTile) {
+        const int tile = min(kFieldTile, n - t0);
+        __syncthreads();  // the previous tile is no longer read
+        for (int q = static_cast<int>(threadIdx.x); q < kFieldGroup * kFieldTile; q += kFieldThreads) {
+            const int j = q / kFieldGroup, g = q % kFieldGroup;  // consecutive threads: one row, conflict-free stores
+            sigma[j][g] = (g < group && j < tile)
+                              ? static_cast<double>(spins[static_cast<size_t>(k0 + g) * spin_stride + t0 + j])
+                              : 0.0;
+        }
+        __syncthreads();
+        for (int j0 = 0; j0 < tile; j0 += kFieldPrefetch) {
+            // the next kFieldPrefetch rows of J, issued before this block of rows is summed
+            double jn[kFieldPrefetch];
+#pragma unroll
+            for (int u = 0; u < kFieldPrefetch; ++u) {
+                const int j = t0 + j0 + kFieldPrefetch + u;
+                jn[u] = j < n ? col[static_cast<size_t>(j) * ld] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < kFieldPrefetch; ++u) {
+                if (j0 + u < tile) {
+                    const double2* row = reinterpret_cast<const double2*>(&sigma[j0 + u][0]);
+#pragma unroll
+                    for (int g2 = 0; g2 < kFieldGroup / 2; ++g2) {
+                        const double2 sg = row[g2];
+                        sum[2 * g2] += jv[u] * sg.x;
+                        sum[2 * g2 + 1] += jv[u] * sg.y;
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kFieldPrefetch; ++u) jv[u] = jn[u];
+        }
     }
+    if (!site) return;
 #pragma unroll
     for (int g = 0; g < kFieldGroup; ++g)
-        if (g < group) fields[(k0 + g) * field_stride + i] = sum[g];
+        if (g < group) fields[static_cast<size_t>(k0 + g) * field_stride + i] = sum[g];
 }
 
-// total_energy: one thread per configuration, sequential over i.
-__global__ void energy_kernel(int n, const int8_t* __restrict__ spins, int64_t spin_stride,
-                              const double* __restrict__ fields, int64_t field_stride, double* __restrict__ out,
-                              int count) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count) return;
+// total_energy (src/physics.cpp:253-259): E = sum over i of 0.5 * s_i * h_i, in site order.  One
+// warp per configuration: the lanes form 32 terms at a time (coalesced loads, the next chunk's
+// issued before this chunk is added) and every lane adds them in order from shared memory, so
+// the sum is the reference's sequential one.
+constexpr int kEnergyWarps = 4;
+__global__ void __launch_bounds__(32 * kEnergyWarps) energy_kernel(int n, const int8_t* __restrict__ spins,
+                                                                   int64_t spin_stride,
+                                                                   const double* __restrict__ fields,
+                                                                   int64_t field_stride, double* __restrict__ out,
+                                                                   int count) {
+    __shared__ double terms[kEnergyWarps][32];
+    const int warp = static_cast<int>(threadIdx.x >> 5), lane = static_cast<int>(threadIdx.x & 31);
+    const int k = static_cast<int>(blockIdx.x) * kEnergyWarps + warp;
+    if (k >= count) return;  // whole warps only: the kernel has no block-wide barrier
+    const int8_t* s = spins + static_cast<size_t>(k) * spin_stride;
+    const double* f = fields + static_cast<size_t>(k) * field_stride;
+    int8_t sn = lane < n ? s[lane] : 0;
+    double fn = lane < n ? f[lane] : 0.0;
     double e = 0.0;
-    for (int i = 0; i < n; ++i)
-        e += 0.5 * static_cast<double>(spins[k * spin_stride + i]) * fields[k * field_stride + i];
-    out[k] = e;
+    for (int base = 0; base < n; base += 32) {
+        terms[warp][lane] = 0.5 * static_cast<double>(sn) * fn;
+        __syncwarp();
+        const int next = base + 32 + lane;  // the next chunk's loads, in flight during the adds
+        sn = next < n ? s[next] : 0;
+        fn = next < n ? f[next] : 0.0;
+        const int m = min(32, n - base);
+        for (int q = 0; q < m; ++q) e += terms[warp][q];
+        __syncwarp();
+    }
+    if (lane == 0) out[k] = e;
 }
 
 // ---- host launchers ------------------------------------------------------------------
@@ -464,11 +522,10 @@ void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream) {
 void compute_fields(const EngineView& v, const int8_t* spins, int64_t spin_stride, double* fields,
                     int64_t field_stride, double* energies, int count, cudaStream_t stream) {
     if (count <= 0) return;
-    const size_t staged = static_cast<size_t>(kFieldGroup) * static_cast<size_t>(v.n);
-    if (!v.csr && count > 1 && staged <= 48 * 1024) {
-        const dim3 grid(static_cast<unsigned>((v.n + 127) / 128),
+    if (!v.csr && count > 1) {
+        const dim3 grid(static_cast<unsigned>((v.n + kFieldThreads - 1) / kFieldThreads),
                         static_cast<unsigned>((count + kFieldGroup - 1) / kFieldGroup));
-        fields_group_kernel<<<grid, 128, staged, stream>>>(v, spins, spin_stride, fields, field_stride, count);
+        fields_group_kernel<<<grid, kFieldThreads, 0, stream>>>(v, spins, spin_stride, fields, field_stride, count);
         check_cuda(cudaGetLastError(), "fields_group_kernel");
     } else {
         const dim3 grid(static_cast<unsigned>((v.n + 127) / 128), static_cast<unsigned>(count));
@@ -476,7 +533,7 @@ void compute_fields(const EngineView& v, const int8_t* spins, int64_t spin_strid
         check_cuda(cudaGetLastError(), "fields_kernel");
     }
     if (energies) {
-        energy_kernel<<<static_cast<unsigned>((count + 127) / 128), 128, 0, stream>>>(
+        energy_kernel<<<static_cast<unsigned>((count + kEnergyWarps - 1) / kEnergyWarps), 32 * kEnergyWarps, 0, stream>>>(
             v.n, spins, spin_stride, fields, field_stride, energies, count);
         check_cuda(cudaGetLastError(), "energy_kernel");
     }

@@ -287,6 +287,8 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_kernel(EngineView v, WalkAr
             continue;
         }
         const int i = static_cast<int>(fast_mod(v.site_mod, q0));
+        // BF16: the site's row scale, loaded before the decision so that an accepted flip does not wait for it
+        const float row_scale = kPrec == WLG_PRECISION_BF16 ? __ldg(v.Jscale + i) : 1.0f;
         const uint32_t slot = head;
         const int8_t si = sp_s[i];
         const double m = -2.0 * static_cast<double>(si);
@@ -316,7 +318,7 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_kernel(EngineView v, WalkAr
         }
         if (accepted) {
             double mm = m;
-            if constexpr (kPrec == WLG_PRECISION_BF16) mm *= static_cast<double>(__ldg(v.Jscale + i));
+            if constexpr (kPrec == WLG_PRECISION_BF16) mm *= row_scale;
             if (!wait_slot(slot)) {
                 failed = true;
                 break;
