@@ -299,11 +299,11 @@ __global__ void fields_kernel(EngineView v, const int8_t* __restrict__ spins, in
 // local_fields of dense couplings for kFieldGroup configurations per block.  Each thread owns
 // one site i and keeps kFieldGroup sums; the J column entries J[j][i] are read kFieldPrefetch
 // rows ahead into registers, and the configurations' spins are staged as doubles (+-1.0) in
-// shared memory, kFieldTile rows at a time, so that a term is one shared-memory broadcast, one
-// multiply and one add.  Every field is still summed sequentially over j with the reference's
+// shared memory, kFieldTile rows at a time, so that a term is one multiply and one add, with one
+// shared-memory broadcast (a double2) per two terms.  Every field is still summed sequentially over j with the reference's
 // operations (sum += J(i, j) * s_j, no contraction), so the result is the one of fields_kernel.
-constexpr int kFieldGroup = 16;
-constexpr int kFieldTile = 256;     // rows j staged per pass (kFieldGroup x kFieldTile doubles = 32 KB)
+constexpr int kFieldGroup = 8;      // configurations per block (16 measured slightly slower: fewer blocks)
+constexpr int kFieldTile = 256;     // rows j staged per pass (kFieldGroup x kFieldTile doubles = 16 KB)
 constexpr int kFieldPrefetch = 8;   // rows of J in flight per thread
 constexpr int kFieldThreads = 128;
 __global__ void __launch_bounds__(kFieldThreads) fields_group_kernel(EngineView v, const int8_t* __restrict__ spins,
