@@ -2,9 +2,15 @@
 //  * x87_mean(total, count) must equal (double)((long double)total / (long double)count),
 //    the reference's histogram mean (src/wang_landau.cpp:349-361);
 //  * fast_mod(x) must equal x % bound (Barrett reduction used by bounded(),
-//    include/wl/rng.hpp:29-36).
+//    include/wl/rng.hpp:29-36);
+//  * rng_step_back must invert Rng::next();
+//  * the sweeps' bin floor: for a bin coordinate 0 <= q < 2^31, the sum q + 2^52 rounded toward
+//    -infinity is 2^52 + floor(q), so its low word is floor(q) (bin_floor in walker_dev.cuh does
+//    the add with __dadd_rd; here the host rounding mode stands in for it).
 // Prints "ok <cases>" or the first mismatch.
+#include <cfenv>
 #include <cinttypes>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 
@@ -61,6 +67,36 @@ int main() {
             return 1;
         }
         ++cases;
+    }
+    // bin floor by a directed-rounding add
+    {
+        std::fesetround(FE_DOWNWARD);
+        for (int k = 0; k < 2000000; ++k) {
+            double q;
+            const uint64_t r = rng.next();
+            switch (k % 4) {
+                case 0: q = static_cast<double>(r >> 33) * 0x1p-20; break;                  // fractional coordinates
+                case 1: q = static_cast<double>(r % 100000); break;                          // exact integers
+                case 2: q = std::nextafter(static_cast<double>(1 + r % 100000), 0.0); break;  // just below an integer
+                default: q = static_cast<double>(r >> 33); break;                            // up to 2^31 - 1
+            }
+            volatile double a = q;
+            volatile double sum = a + 0x1p52;
+            const double s = sum;
+            uint64_t bits;
+            std::memcpy(&bits, &s, 8);
+            const uint32_t low = static_cast<uint32_t>(bits & 0xffffffffULL);
+            std::fesetround(FE_TONEAREST);
+            const uint32_t want = static_cast<uint32_t>(std::floor(q));
+            std::fesetround(FE_DOWNWARD);
+            if (low != want) {
+                std::fesetround(FE_TONEAREST);
+                std::printf("bin floor mismatch q=%a low=%u want=%u\n", q, low, want);
+                return 1;
+            }
+            ++cases;
+        }
+        std::fesetround(FE_TONEAREST);
     }
     std::printf("ok %" PRIu64 "\n", cases);
     return 0;

@@ -58,9 +58,10 @@ def test_struct_layouts_match_header(tmp_path):
 
 @pytest.mark.skipif(shutil.which("g++") is None, reason="g++ not available")
 def test_kernel_integer_helpers_exact(tmp_path):
-    """x87_mean reproduces the reference's long-double histogram mean; fast_mod is exact."""
+    """x87_mean reproduces the reference's long-double histogram mean; fast_mod, the generator's
+    step back and the add-based bin floor are exact."""
     exe = tmp_path / "host_math_check"
-    subprocess.run(["g++", "-std=c++17", "-O2", "-I/usr/local/cuda/include",
+    subprocess.run(["g++", "-std=c++17", "-O2", "-frounding-math", "-I/usr/local/cuda/include",
                     str(ROOT / "tests" / "native" / "host_math_check.cpp"), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True)
     assert out.returncode == 0 and out.stdout.startswith("ok"), out.stdout
