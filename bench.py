@@ -170,13 +170,26 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
             attempted += t["attempted"]
             accepted += t["accepted"]
         torch.cuda.synchronize()
-    # per-kernel device times for the roofline: the same epochs launched one kernel at a
-    # time with CUDA events around every launch (after the timed region)
-    kernel_epochs = min(epochs, 50)
-    flush_l2(torch, flush)
-    torch.cuda.synchronize()
-    kt = eng.time_epochs(kernel_epochs)
-    walk_ms, exch_ms = kt["walk_ms"], kt["exchange_ms"]
+    # per-kernel device times for the roofline, on the timed epochs themselves: a second
+    # engine with the same system and seed replays the warm-up and then exactly the timed
+    # steps' epochs, launched one kernel at a time with CUDA events around every launch.  The
+    # trajectories are deterministic, so these are the same attempts (checked below).
+    twin = E.Engine(system, config)
+    for _ in range(args.warmup):
+        twin.time_epochs(epochs)
+    walk_ms = exch_ms = 0.0
+    kt = {"epochs": 0, "attempted": 0, "accepted": 0}
+    for _ in range(args.steps):
+        flush_l2(torch, flush)
+        torch.cuda.synchronize()
+        t = twin.time_epochs(epochs)
+        walk_ms += t["walk_ms"]
+        exch_ms += t["exchange_ms"]
+        for key in kt:
+            kt[key] += t[key]
+    twin.close()
+    if (kt["attempted"], kt["accepted"]) != (attempted, accepted):
+        raise RuntimeError("the kernel-timing replay did not repeat the timed epochs")
     if dist:
         dist.barrier()
     clock = clocks.summary()
@@ -272,8 +285,10 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
                          "kernel": "sweep_dense_split_kernel<8, pow2 width> (FP64 dense J)", "peak_source": peaks["source"],
                          "bytes_per_launch": bytes_per_launch, "launch_ms": launch_s * 1e3,
                          "acceptance": kt["accepted"] / max(1, kt["attempted"]),
-                         "kernel_timing": f"{k_launches} epochs launched one kernel at a time with CUDA events "
-                                          f"around each launch, after the timed region"},
+                         "kernel_timing": f"the {k_launches} timed epochs (warm-up excluded), replayed after the "
+                                          f"timed region by a second engine with the same seed, one kernel at a time "
+                                          f"with CUDA events around each launch; same attempts and accepted flips "
+                                          f"as the timed region (checked)"},
             "gpu_launches": 2 * launches,
             "wall_clock_attempts_per_s": graph_rate,
             "clocks": clock,
@@ -421,7 +436,41 @@ def batched_instances_line(count: int = 256, epochs: int = 32) -> dict:
             "epochs": epochs, "setup_s": setup_s, "timing": "wall clock, host synchronisation included"}
 
 
-def csr_batched_line(epochs: int = 40, pilot_mcs: float = 20.0) -> dict:
+def csr_cpu_baseline(system, config, attempts: int = 2_000_000) -> dict:
+    """The reference on the CSR configuration, in steady state: one reference walker
+    (WangLandauWalker, compiled from the reference's sources) on the same system, grid and a
+    window in the middle of the range.  Its construction (CsrCouplings built from the
+    geometry, then local_fields and total_energy, which read J through Couplings::at and so
+    cost O(N^2 z), OpenMP over rows) is timed and reported apart; then `attempts` attempts are
+    timed on one core.  The full configuration (1024 walkers) cannot run on the host in a
+    bounded sample: construction alone is this cost once per walker."""
+    from oracle.oracle import Reference
+    ref = Reference()
+    threads = ref.set_threads(os.cpu_count() or 1)
+    bins = int(round((config.emax - config.emin) / config.bin_width))
+    middle = int(np.floor((0.0 - config.emin) / config.bin_width))
+    window = (max(0, middle - 30), min(bins, middle + 30))
+    t0 = time.perf_counter()
+    walker = ref.walker(system, 0, config.emin, config.emax, config.bin_width, window, config.wl, config.seed)
+    construct_s = time.perf_counter() - t0
+    try:
+        walker.run_attempts(attempts // 10)  # warm
+        a0 = walker.counters()[0]
+        t0 = time.perf_counter()
+        walker.run_attempts(attempts)
+        dt = time.perf_counter() - t0
+        acc = walker.counters()
+        rate = (acc[0] - a0) / dt
+    finally:
+        walker.close()
+    return {"value": rate, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"one reference walker on the same system and grid, window bins {window[0]}-{window[1]}, "
+                      f"{attempts} attempts timed on one core after construction",
+            "construction_s": construct_s, "construction_threads": threads,
+            "acceptance": acc[1] / max(1, acc[0])}
+
+
+def csr_batched_line(epochs: int = 40, pilot_mcs: float = 20.0, with_cpu_baseline: bool = True) -> dict:
     """The CSR configuration: 32x32x32 periodic simple cubic (N = 32768), cutoff 3.0 (122
     neighbours), easy axes +z, FP32 CSR values with FP64 fields, 64 adaptive windows x 16
     walkers = 1024 walkers.  The windows and the walkers' seeds come from two adaptive-window
@@ -451,8 +500,14 @@ def csr_batched_line(epochs: int = 40, pilot_mcs: float = 20.0) -> dict:
         e.time_run(8)
         t = e.time_run(epochs)
         rep = e.precision_report()
+    cpu = None
+    if with_cpu_baseline:
+        try:
+            cpu = csr_cpu_baseline(system, c)
+        except Exception as exc:  # reported, never fatal to the line
+            cpu = {"error": str(exc)}
     return {"value": t["attempted"] / (t["total_ms"] / 1e3), "unit": UNIT, "walkers": 1024, "spins": system.size(),
-            "neighbours": 122, "couplings": "fp32 CSR, fp64 fields",
+            "cpu_baseline": cpu, "neighbours": 122, "couplings": "fp32 CSR, fp64 fields",
             "windows": {"count": len(windows), "adaptive_rounds": 2, "pilot_mcs_per_round": pilot_mcs,
                         "pilot_s": pilot_s, "min_bins": min(widths), "max_bins": max(widths),
                         "seeded_walkers": sum(1 for x in seeds if x is not None)},
@@ -574,35 +629,60 @@ def time_to_converge(value: float, cpu_value: float, active_bins: float, window_
     return out
 
 
+# The reference's own program, compiled unmodified from its sources by oracle/Makefile, and
+# the workload's geometry in the reference's CSV format (written from
+# simple_cubic_random(8, 8, 8, seed=1); tests/test_bench_workload.py checks that the file
+# holds exactly the doubles the generator gives).
+REFERENCE_WL_RUN = ROOT / "oracle" / "_ref" / "wl_run"
+WORKLOAD_CSV = ROOT / "oracle" / "workloads" / "dense_rewl_8x8x8_seed1.csv"
+
+
+def reference_wl_run_command(mcs: float, seed: int, output_prefix: str) -> list:
+    """wl_run's command line for the dense REWL workload (the options of src/io.cpp:300-361)."""
+    return [str(REFERENCE_WL_RUN), "--geometry", str(WORKLOAD_CSV), "--box-x", "8", "--box-y", "8", "--box-z", "8",
+            "--periodic", "true", "--coupling", "1", "--emin", repr(EMIN), "--emax", repr(EMAX),
+            "--bin-width", repr(WIDTH), "--windows", "16", "--walkers", "8", "--overlap", "0.75",
+            "--exchange-interval-mcs", "1", "--max-mcs", f"{mcs:g}", "--seed", str(seed), "--output", output_prefix]
+
+
+def parse_wl_run_summary(stdout: str) -> dict:
+    """The key=value summary line wl_run prints after run_rewl (apps/wl_run.cpp:190-197)."""
+    for line in stdout.splitlines():
+        if line.startswith("attempted_flips="):
+            return dict(item.split("=", 1) for item in line.split())
+    raise RuntimeError("wl_run printed no summary line")
+
+
 def reference_rate(mcs: float, threads: int, seed: int = 1):
-    from oracle.oracle import Reference
-    ref = Reference()
-    used = ref.set_threads(threads)
-    system, config = make_workload(seed=seed)
-    config.max_mcs = mcs
-    config.resolved_spin_count = 0
-    config.resolve_mcs(system.size())
-    t0 = time.perf_counter()
-    r = ref.run_rewl(system, config)
-    dt = time.perf_counter() - t0
-    return r.attempted, dt, used
+    """One run of the reference's unmodified wl_run on the workload: (attempts, seconds of
+    run_rewl as wl_run measures it -- walker construction included, J build and output
+    excluded, threads)."""
+    with tempfile.TemporaryDirectory() as d:
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        res = subprocess.run(reference_wl_run_command(mcs, seed, str(Path(d) / "ref")), capture_output=True,
+                             text=True, env=env, timeout=1800)
+    if res.returncode not in (0, 2):  # 2 = max-mcs reached before the final factor
+        raise RuntimeError(f"wl_run failed ({res.returncode}): {res.stderr.strip()[-500:]}")
+    summary = parse_wl_run_summary(res.stdout)
+    return int(summary["attempted_flips"]), float(summary["elapsed_seconds"]), threads
 
 
 def cpu_baseline(sample_mcs: float) -> dict:
     threads = os.cpu_count() or 1
     attempted, dt, used = reference_rate(sample_mcs, threads)
     return {"value": attempted / dt, "unit": UNIT, "cores": used, "kind": "reference",
-            "sample": f"reference run_rewl (oracle/_ref, built from the reference sources, OpenMP) on the same "
-                      f"system and 16x8 walkers, {sample_mcs:g} MCS per walker including walker construction, "
-                      f"{dt:.2f} s"}
+            "sample": f"the reference's wl_run (oracle/_ref, compiled unmodified from its sources, OpenMP over walkers) "
+                      f"on the same system (CSV) and 16x8 walkers, {sample_mcs:g} MCS per walker; run_rewl time as "
+                      f"wl_run reports it, walker construction included: {dt:.2f} s"}
 
 
 def run_reference(args, rank: int) -> None:
+    """The reference arm: the reference's own wl_run program (its public command line and
+    stock code path, nothing of this repository's engine) on the workload, every host core."""
     if rank != 0:
         return
-    from oracle.oracle import reference_available
-    if not reference_available():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libwlref.so was not built"}))
+    if not REFERENCE_WL_RUN.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/wl_run was not built"}))
         return
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
@@ -615,9 +695,9 @@ def run_reference(args, rank: int) -> None:
         total_t += dt
         total_a += a
     value = total_a / total_t
-    sample = (f"reference run_rewl per step (oracle/_ref, compiled from the reference sources, OpenMP over walkers) "
-              f"on the same system and 16x8 walkers, {args.reference_step_mcs:g} MCS per walker per step, walker "
-              f"construction included")
+    sample = (f"the reference's wl_run per step (oracle/_ref, compiled unmodified from its sources, OpenMP over "
+              f"walkers) on the same system (CSV) and 16x8 walkers, {args.reference_step_mcs:g} MCS per walker per "
+              f"step; run_rewl time as wl_run reports it, walker construction included")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * total_t / args.steps, "higher_is_better": True,

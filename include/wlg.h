@@ -246,9 +246,11 @@ wlg_status wlg_local_fields(const wlg_system* system, const int8_t* spins, uint6
  * staging live in one static device array of 18 MiB that every GPU loading this library
  * keeps until the process exits.  Limits: dense systems only (cutoff 0), n <= 1024 sites,
  * count <= 65536 configurations and count * n <= 1048576; larger inputs return
- * WLG_ERR_INVALID_ARGUMENT with the limit in the message.  The first call on a device looks
- * up the array's device address and should come before any stream capture.  Calls share
- * the array: calls that overlap on the GPU race. */
+ * WLG_ERR_INVALID_ARGUMENT with the limit in the message.  Every call looks up the array's
+ * device address on the current device; the first call on a device loads the library's
+ * device code and should come before any stream capture.  Work runs on the legacy default
+ * stream, so no call may run while another thread holds a global-mode stream capture.
+ * Calls share the array: calls that overlap on the GPU race. */
 wlg_status wlg_local_fields_noalloc(const wlg_system* system, const int8_t* spins,
                                     uint64_t count, double* fields, double* energies);
 

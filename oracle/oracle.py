@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 import subprocess
 from dataclasses import dataclass
 from pathlib import Path
@@ -34,9 +35,18 @@ P = C.POINTER
 _u64, _i64, _i32, _dbl, _vp, _cp, _sz = C.c_uint64, C.c_int64, C.c_int32, C.c_double, C.c_void_p, C.c_char_p, C.c_size_t
 
 
+# Where the reference's source tree is read from when it is present (the build container);
+# WL_REFERENCE_DIR overrides it.  Machines without it use the prebuilt oracle/_ref files.
+REFERENCE_SOURCES = Path(os.environ.get("WL_REFERENCE_DIR", "/root/reference"))
+
+
 def build() -> None:
-    """Runs oracle/Makefile (compiles the restatement; the reference too when present)."""
-    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    """Runs oracle/Makefile (compiles the restatement; the reference too when its sources
+    are present)."""
+    cmd = ["make", "-s", "-C", str(HERE)]
+    if (REFERENCE_SOURCES / "src" / "physics.cpp").exists():
+        cmd.append(f"REF={REFERENCE_SOURCES}")
+    subprocess.run(cmd, check=True)
 
 
 def reference_available() -> bool:

@@ -984,8 +984,27 @@ static int validate_config(const wlg_run_config* c, uint64_t bins_checked, char*
     return 0;
 }
 
+/* The engine's FP32-couplings form (an extension; the reference stores J in FP64 only): walkers
+ * are constructed from the FP64 couplings, then every accepted flip adds the FP32-rounded
+ * coupling (update_value).  The engine's periodic FP64 recompute and resync have no restatement
+ * here, so a run must end before the first one is due; BF16 is not restated. */
+static int check_precision(const wlg_run_config* cfg, char* err, size_t len) {
+    if (cfg->coupling_precision == WLG_PRECISION_FP64) return 0;
+    if (cfg->coupling_precision != WLG_PRECISION_FP32) {
+        set_err(err, len, "the oracle restates FP64 and FP32 couplings only");
+        return 1;
+    }
+    if (cfg->recompute_interval_attempts != 0 &&
+        (cfg->max_attempts == 0 || cfg->max_attempts >= cfg->recompute_interval_attempts)) {
+        set_err(err, len, "the oracle restates FP32 runs only up to their first FP64 recompute");
+        return 1;
+    }
+    return 0;
+}
+
 orc_result* orc_run_rewl(const orc_couplings* c, const wlg_run_config* cfg, char* err, size_t len) {
     if (validate_config(cfg, 0, err, len)) return NULL;
+    if (check_precision(cfg, err, len)) return NULL;
     uint64_t bins = 0;
     orc_grid_bins(cfg->emin, cfg->emax, cfg->bin_width, &bins);
     const uint64_t nw = cfg->windows, wpw = cfg->walkers_per_window, total = nw * wpw, n = c->n;
@@ -1014,6 +1033,9 @@ orc_result* orc_run_rewl(const orc_couplings* c, const wlg_run_config* cfg, char
                 return NULL;
             }
         }
+    /* FP32 couplings: the constructors above used FP64; the updates from here on use FP32 */
+    const int saved_update_fp32 = c->update_fp32;
+    if (cfg->coupling_precision == WLG_PRECISION_FP32) ((orc_couplings*)c)->update_fp32 = 1;
     const int checkpointing = cfg->checkpoint_path && cfg->checkpoint_path[0] && nw == 1 && wpw == 1;
     if (checkpointing) {
         int8_t* sp = malloc(n); double* fl = malloc(n * 8); double* lg = malloc(bins * 8);
@@ -1078,6 +1100,7 @@ orc_result* orc_run_rewl(const orc_couplings* c, const wlg_run_config* cfg, char
         done = all_frozen || limit_reached;
     }
     free(last_check);
+    ((orc_couplings*)c)->update_fp32 = saved_update_fp32;
     if (status) {
         for (uint64_t q = 0; q < total; ++q) orc_walker_destroy(ws[q]);
         free(ws); free(windows); orc_result_destroy(r);

@@ -61,21 +61,50 @@ void require_device() {
 
 }  // namespace
 
-cudaStream_t pool_stream() {
+namespace {
+
+struct DevicePool {
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+};
+
+// The library's own stream and memory pool on the current device, created once.  The pool
+// is private: the device's default pool, which other code in the process may use through
+// cudaMallocAsync, keeps its own attributes.
+const DevicePool& device_pool() {
     static std::mutex mu;
-    static cudaStream_t streams[64] = {};
+    static DevicePool pools[64];
     int device = 0;
     check_cuda(cudaGetDevice(&device), "cudaGetDevice");
-    if (device >= 64) throw WlgError(WLG_ERR_DEVICE, "device index beyond 63");
+    if (device < 0 || device >= 64) throw WlgError(WLG_ERR_DEVICE, "device index beyond 63");
     std::lock_guard<std::mutex> lock(mu);
-    if (!streams[device]) {
+    DevicePool& d = pools[device];
+    if (!d.pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
         cudaMemPool_t pool = nullptr;
-        check_cuda(cudaDeviceGetDefaultMemPool(&pool, device), "cudaDeviceGetDefaultMemPool");
+        check_cuda(cudaMemPoolCreate(&pool, &props), "cudaMemPoolCreate");
         uint64_t keep = ~0ULL;
         check_cuda(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
-        check_cuda(cudaStreamCreateWithFlags(&streams[device], cudaStreamNonBlocking), "cudaStreamCreate");
+        check_cuda(cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        d.pool = pool;
     }
-    return streams[device];
+    return d;
+}
+
+}  // namespace
+
+cudaStream_t pool_stream() { return device_pool().stream; }
+
+void* pool_allocate(size_t bytes) {
+    const DevicePool& d = device_pool();
+    void* ptr = nullptr;
+    check_cuda(cudaMallocFromPoolAsync(&ptr, bytes, d.pool, d.stream), "cudaMallocFromPoolAsync");
+    check_cuda(cudaStreamSynchronize(d.stream), "allocation");
+    return ptr;
 }
 
 Engine::Engine(const wlg_system& system, const wlg_run_config& c) : cfg_(c) {

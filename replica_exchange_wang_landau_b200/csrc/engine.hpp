@@ -26,12 +26,14 @@ inline void check_cuda(cudaError_t e, const char* what) {
         throw WlgError(WLG_ERR_DEVICE, std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e));
 }
 
-// The stream on which the current device's buffers are allocated and freed from its default
-// memory pool.  Created once per device and kept; the pool keeps freed memory (release
-// threshold = unlimited) so that creating and destroying engines costs no driver-level
-// allocation after the first one.  (cudaMalloc / cudaFree took up to hundreds of ms per
-// engine destruction.)
+// The stream on which the current device's buffers are allocated and freed, from a memory
+// pool of the library's own (not the device's default pool).  Created once per device and
+// kept; the pool keeps freed memory (release threshold = unlimited) so that creating and
+// destroying engines costs no driver-level allocation after the first one.  (cudaMalloc /
+// cudaFree took up to hundreds of ms per engine destruction.)
 cudaStream_t pool_stream();
+// `bytes` from that pool, complete when the call returns.
+void* pool_allocate(size_t bytes);
 
 // Owning device allocation, stream-ordered on pool_stream().  The allocation is complete
 // before allocate() returns, so any stream may use it.  The owner must have finished every
@@ -54,11 +56,9 @@ struct DeviceBuffer {
     void allocate(size_t b) {
         release();
         if (b == 0) b = 16;
-        cudaStream_t s = pool_stream();
-        check_cuda(cudaMallocAsync(&ptr, b, s), "cudaMallocAsync");
-        stream = s;
+        ptr = pool_allocate(b);
+        stream = pool_stream();
         bytes = b;
-        check_cuda(cudaStreamSynchronize(s), "allocation");
     }
     void release() {
         if (ptr) {

@@ -9,14 +9,16 @@
 //
 // The array is a file-scope __device__ object, so every GPU that loads the library holds
 // it until the process exits (kScratchBytes, 18 MiB).  Host code may not use its name as a
-// device address; the device address is looked up once per device with
-// cudaGetSymbolAddress, with that device current, on the first call made on that device.
-// That first call should therefore come before any stream capture.  All calls share the
-// array and it keeps the last call's contents: the regions that must start at zero (the
-// coupling matrix with its padding, the error flag) are cleared on every call, and calls
-// that overlap on the GPU (from several host threads at once) race on the array.  Work is
-// issued on the legacy default stream.
-#include <mutex>
+// device address; every call looks the device address up with cudaGetSymbolAddress, with
+// the calling thread's device current (cheap, and it allocates nothing).  Looking it up on
+// every call rather than caching it keeps the address valid after the host resets the
+// device (cudaDeviceReset reloads the module at a new address).  The first call on a device
+// loads the library's device code and should come before any stream capture.  All calls
+// share the array and it keeps the last call's contents: the regions that must start at
+// zero (the coupling matrix with its padding, the error flag) are cleared on every call,
+// and calls that overlap on the GPU (from several host threads at once) race on the array.
+// Work is issued on the legacy default stream, which synchronises with blocking streams, so
+// no call may run while another thread holds a global-mode stream capture.
 
 #include "engine.hpp"
 
@@ -38,30 +40,18 @@ constexpr size_t kOffFields = kOffSpins + kMaxValues;
 constexpr size_t kOffEnergies = kOffFields + kMaxValues * 8;
 constexpr size_t kScratchBytes = kOffEnergies + kMaxConfigs * 8;  // 18,022,656 bytes
 
-constexpr int kMaxDevices = 64;
-
 }  // namespace
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 namespace {
 
-std::mutex g_setup_mutex;
-unsigned char* g_scratch_address[kMaxDevices] = {};
-
-// The device address of g_noalloc_scratch on the current device (looked up once).
+// The device address of g_noalloc_scratch on the current device, looked up on every call.
 unsigned char* scratch_on_current_device() {
-    int device = 0;
-    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
-    if (device < 0 || device >= kMaxDevices) throw WlgError(WLG_ERR_DEVICE, "device index out of range");
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_address[device]) {
-        void* p = nullptr;
-        check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
-        if (!p) throw WlgError(WLG_ERR_DEVICE, "cudaGetSymbolAddress returned a null address");
-        g_scratch_address[device] = static_cast<unsigned char*>(p);
-    }
-    return g_scratch_address[device];
+    void* p = nullptr;
+    check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+    if (!p) throw WlgError(WLG_ERR_DEVICE, "cudaGetSymbolAddress returned a null address");
+    return static_cast<unsigned char*>(p);
 }
 
 }  // namespace

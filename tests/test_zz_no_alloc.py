@@ -30,12 +30,13 @@ def _system(dims, seed, box=None, periodic=True):
     return System(g, 0.8, 0.0)
 
 
-def _call(fn, system, spins):
+def _call(fn, system, spins, with_energies=True):
     fields = np.full(spins.shape, np.nan)
     energies = np.full(spins.shape[0], np.nan)
     s = system._struct()
+    energy_ptr = energies.ctypes.data_as(C.POINTER(C.c_double)) if with_energies else None
     status = fn(C.byref(s), spins.ctypes.data_as(C.POINTER(C.c_int8)), spins.shape[0],
-                fields.ctypes.data_as(C.POINTER(C.c_double)), energies.ctypes.data_as(C.POINTER(C.c_double)))
+                fields.ctypes.data_as(C.POINTER(C.c_double)), energy_ptr)
     return status, fields, energies
 
 
@@ -51,6 +52,22 @@ def test_no_alloc_matches_allocating_entry_point_on_two_calls():
         assert st_a == 0 and st_b == 0, lib.wlg_last_error()
         assert np.array_equal(fa.view(np.uint64), fb.view(np.uint64))
         assert np.array_equal(ea.view(np.uint64), eb.view(np.uint64))
+
+
+def test_no_alloc_single_configuration_and_no_energies():
+    # count == 1 takes the one-configuration field kernel; energies may be NULL
+    lib = load_library()
+    rng = np.random.default_rng(11)
+    for system, with_energies in [(_system((6, 6, 6), 8), True), (_system((4, 4, 2), 9, box=(4.0, 4.0, 0.0)), False)]:
+        spins = np.ascontiguousarray(rng.choice(np.array([-1, 1], np.int8), size=(1, system.size())))
+        st_a, fa, ea = _call(lib.wlg_local_fields, system, spins, with_energies)
+        st_b, fb, eb = _call(lib.wlg_local_fields_noalloc, system, spins, with_energies)
+        assert st_a == 0 and st_b == 0, lib.wlg_last_error()
+        assert np.array_equal(fa.view(np.uint64), fb.view(np.uint64))
+        if with_energies:
+            assert np.array_equal(ea.view(np.uint64), eb.view(np.uint64))
+        else:
+            assert np.isnan(eb).all()
 
 
 def test_no_alloc_rejects_inputs_beyond_its_limits():
