@@ -65,6 +65,23 @@ typedef struct wlg_system {
     double cutoff;            /* > 0 selects the CSR backend with |r| <= cutoff         */
 } wlg_system;
 
+/* Prebuilt couplings: the J of a wl::Couplings object (include/wl/physics.hpp:41-49) as
+ * Couplings::at(i, j) exports it, for callers that hold couplings rather than a geometry
+ * (run_rewl takes std::shared_ptr<const Couplings>, include/wl/parallel.hpp:35-36).  Dense
+ * (DenseCouplings, src/physics.cpp:172-188): `dense` is the n x n row-major matrix and the CSR
+ * members are unused.  CSR (CsrCouplings, src/physics.cpp:197-229): `dense` is NULL and
+ * row_offsets[n+1] / columns[nnz] / values[nnz] hold each row's stored couplings by ascending
+ * column.  Either form must be symmetric with a zero diagonal and finite values, as both
+ * reference backends are; otherwise creation fails with WLG_ERR_INVALID_ARGUMENT. */
+typedef struct wlg_couplings {
+    uint64_t n;                  /* number of sites                                        */
+    const double* dense;         /* n x n, or NULL for the CSR form                        */
+    uint64_t nnz;                /* CSR: stored couplings                                  */
+    const uint64_t* row_offsets; /* CSR: n + 1 offsets into columns / values               */
+    const uint64_t* columns;     /* CSR: column of each stored coupling                    */
+    const double* values;        /* CSR: value of each stored coupling                     */
+} wlg_couplings;
+
 /* wl::WlParameters (include/wl/wang_landau.hpp:40-56), field for field. */
 typedef struct wlg_wl_parameters {
     double flatness;
@@ -261,6 +278,12 @@ wlg_status wlg_local_fields_noalloc(const wlg_system* system, const int8_t* spin
  * the reference would (src/parallel.cpp:354-360). */
 wlg_status wlg_engine_create(const wlg_system* system, const wlg_run_config* config,
                              wlg_engine** engine);
+/* The same engine from prebuilt couplings instead of a geometry: run_rewl's own inputs
+ * (std::shared_ptr<const Couplings> + RunConfig, include/wl/parallel.hpp:35-36).  The dense
+ * form runs the dense sweeps, the CSR form the CSR sweeps, exactly as an engine created from
+ * the geometry those couplings came from. */
+wlg_status wlg_engine_create_from_couplings(const wlg_couplings* couplings, const wlg_run_config* config,
+                                            wlg_engine** engine);
 void wlg_engine_destroy(wlg_engine* engine);
 /* The epoch loop of run_rewl (src/parallel.cpp:376-534) until every walker is frozen or
  * the attempt limit is reached. */
@@ -311,6 +334,13 @@ wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block,
  * instead (same results); for other engines the call changes nothing.  No counterpart in
  * the reference. */
 wlg_status wlg_engine_set_window_sweep(wlg_engine* engine, int32_t enabled);
+/* Failure injection, for tests of the bounded device waits (no counterpart in the reference):
+ * from the next epoch on, the draw-producer warps of the split sweep (dense systems up to 1024
+ * sites) and of the single-window sweep publish no draws, so every walker's wait for its first
+ * draws runs to its limit, the walker records WLG_ERR_TIMEOUT without writing its state back,
+ * and the run call returns WLG_ERR_TIMEOUT.  Nothing faults and the device stays usable; the
+ * engine itself is finished and should be destroyed.  Other sweeps are not affected. */
+wlg_status wlg_engine_inject_wait_timeout(wlg_engine* engine);
 /* 1 when the engine runs its epochs with the single-window kernel, else 0. */
 int32_t wlg_engine_window_sweep(const wlg_engine* engine);
 /* The drift report of a mixed-precision run (all zero for FP64 couplings).  No counterpart
@@ -322,6 +352,15 @@ wlg_status wlg_engine_precision_report(wlg_engine* engine, wlg_precision_report*
  * reference, whose walkers start from log g = 0 and ln f = 1; the learned warm start
  * (replica_exchange_wang_landau_b200/warmstart.py) supplies the estimate. */
 wlg_status wlg_engine_warm_start(wlg_engine* engine, const double* log_g, double factor);
+/* The same warm start, continuing the 1/t schedule instead of restarting it: each walker counts
+ * round(window bins / factor) attempts as already made, so that in the 1/t stage its factor is
+ * f = active / (attempted + offset) (update_inverse_time_factor and begin_next_iteration,
+ * src/wang_landau.cpp:309-315, 389-409, with the offset added to attempted).  Under the
+ * reference's rule (offset 0) the first check after a warm start at a small ln f switches to
+ * 1/t with f = active / attempted, far above the start's factor early in a run, which discards
+ * the warm start; with the offset f starts at the warm start's factor and falls as 1/t from
+ * there.  An extension with no counterpart in the reference. */
+wlg_status wlg_engine_warm_start_continue(wlg_engine* engine, const double* log_g, double factor);
 uint64_t wlg_engine_walkers(const wlg_engine* engine);
 uint64_t wlg_engine_bins(const wlg_engine* engine);
 uint64_t wlg_engine_spins(const wlg_engine* engine);

@@ -5,12 +5,12 @@ run_rewl and everything under it -- implemented as sm_100a CUDA kernels behind t
 in include/wlg.h.  Importing the package loads libwlg.so; there is no CPU fallback.
 """
 from ._abi import LIBRARY_PATH, load_library
-from .engine import (DosFragment, Engine, Geometry, InitializationError, InvalidArgument, RewlResult, RunConfig,
+from .engine import (Couplings, DosFragment, Engine, Geometry, InitializationError, InvalidArgument, RewlResult, RunConfig,
                      Snapshot, System, WlgError, WlParameters, attempts_from_mcs, grid_bins, grid_index,
                      load_checkpoint, partition_windows, run_rewl, save_checkpoint)
 
 __all__ = [
-    "LIBRARY_PATH", "load_library", "DosFragment", "Engine", "Geometry", "InitializationError", "InvalidArgument",
+    "LIBRARY_PATH", "load_library", "Couplings", "DosFragment", "Engine", "Geometry", "InitializationError", "InvalidArgument",
     "RewlResult", "RunConfig", "Snapshot", "System", "WlgError", "WlParameters", "attempts_from_mcs", "grid_bins",
     "grid_index", "load_checkpoint", "partition_windows", "run_rewl", "save_checkpoint",
 ]

@@ -41,6 +41,17 @@ class wlg_system(C.Structure):
     ]
 
 
+class wlg_couplings(C.Structure):
+    _fields_ = [
+        ("n", C.c_uint64),
+        ("dense", C.POINTER(C.c_double)),
+        ("nnz", C.c_uint64),
+        ("row_offsets", C.POINTER(C.c_uint64)),
+        ("columns", C.POINTER(C.c_uint64)),
+        ("values", C.POINTER(C.c_double)),
+    ]
+
+
 class wlg_wl_parameters(C.Structure):
     _fields_ = [
         ("flatness", C.c_double),
@@ -226,6 +237,7 @@ class wlg_snapshot(C.Structure):
 
 STRUCTS = {
     "wlg_system": wlg_system,
+    "wlg_couplings": wlg_couplings,
     "wlg_wl_parameters": wlg_wl_parameters,
     "wlg_run_config": wlg_run_config,
     "wlg_histogram_statistics": wlg_histogram_statistics,
@@ -262,7 +274,9 @@ SIGNATURES = {
     "wlg_local_fields": (_i32, [P(wlg_system), P(C.c_int8), _u64, P(_dbl), P(_dbl)]),
     "wlg_local_fields_noalloc": (_i32, [P(wlg_system), P(C.c_int8), _u64, P(_dbl), P(_dbl)]),
     "wlg_engine_create": (_i32, [P(wlg_system), P(wlg_run_config), P(_vp)]),
+    "wlg_engine_create_from_couplings": (_i32, [P(wlg_couplings), P(wlg_run_config), P(_vp)]),
     "wlg_engine_destroy": (None, [_vp]),
+    "wlg_engine_inject_wait_timeout": (_i32, [_vp]),
     "wlg_engine_run": (_i32, [_vp, P(wlg_run_totals)]),
     "wlg_engine_run_epochs": (_i32, [_vp, _u64, P(_u64), P(_i32)]),
     "wlg_engine_totals": (_i32, [_vp, P(wlg_run_totals)]),
@@ -273,6 +287,7 @@ SIGNATURES = {
     "wlg_engine_load_run": (_i32, [_vp, C.c_char_p]),
     "wlg_engine_precision_report": (_i32, [_vp, P(wlg_precision_report)]),
     "wlg_engine_warm_start": (_i32, [_vp, P(_dbl), _dbl]),
+    "wlg_engine_warm_start_continue": (_i32, [_vp, P(_dbl), _dbl]),
     "wlg_stitch_dos": (_i32, [_dbl, _dbl, _dbl, P(wlg_fragment_view), _u64, _i32, _u64, P(_dbl), P(_u64), P(_dbl),
                                P(C.c_uint8), P(wlg_join_quality), P(_i32)]),
     "wlg_write_dos_csv": (_i32, [C.c_char_p, _dbl, _dbl, _u64, P(_dbl), P(_u64), P(_dbl), P(C.c_uint8)]),

@@ -303,6 +303,16 @@ wlg_status wlg_engine_create(const wlg_system* system, const wlg_run_config* con
     });
 }
 
+wlg_status wlg_engine_create_from_couplings(const wlg_couplings* couplings, const wlg_run_config* config,
+                                            wlg_engine** engine) {
+    return guarded([&] {
+        if (!couplings || !config || !engine) throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null argument");
+        *engine = nullptr;
+        auto* impl = new wlg::Engine(*couplings, *config);
+        *engine = new wlg_engine{impl};
+    });
+}
+
 void wlg_engine_destroy(wlg_engine* engine) {
     if (!engine) return;
     if (engine->impl) cudaSetDevice(engine->impl->device);
@@ -314,6 +324,11 @@ void wlg_engine_destroy(wlg_engine* engine) {
     if (!(engine) || !(engine)->impl) return fail(WLG_ERR_INVALID_ARGUMENT, "null engine");  \
     if (cudaSetDevice((engine)->impl->device) != cudaSuccess)                                    \
         return fail(WLG_ERR_DEVICE, "cannot select the engine's CUDA device");
+
+wlg_status wlg_engine_inject_wait_timeout(wlg_engine* engine) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] { engine->impl->inject_wait_timeout(); });
+}
 
 wlg_status wlg_engine_run(wlg_engine* engine, wlg_run_totals* totals) {
     WLG_ENGINE_GUARD(engine)
@@ -378,6 +393,11 @@ wlg_status wlg_engine_precision_report(wlg_engine* engine, wlg_precision_report*
 wlg_status wlg_engine_warm_start(wlg_engine* engine, const double* log_g, double factor) {
     WLG_ENGINE_GUARD(engine)
     return guarded([&] { engine->impl->warm_start(log_g, factor); });
+}
+
+wlg_status wlg_engine_warm_start_continue(wlg_engine* engine, const double* log_g, double factor) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] { engine->impl->warm_start(log_g, factor, true); });
 }
 
 wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block, int32_t epochs_per_graph) {

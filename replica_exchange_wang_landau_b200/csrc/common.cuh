@@ -239,7 +239,10 @@ struct alignas(16) WalkerState {
     int32_t window;        // window index
     int32_t rt_state;      // round-trip state machine
     int32_t rep_pending;   // representatives must be refreshed before the next batch
-    int32_t pad[2];
+    // 1/t stage: attempts counted as made before this run, f = active / (attempted +
+    // time_offset).  0 is the reference's rule; a warm start that continues the schedule
+    // (wlg_engine_warm_start_continue) sets window bins / ln f of the start.
+    uint64_t time_offset;
 };
 
 // Run-wide control block written by the kernels and read by the host.
@@ -275,7 +278,7 @@ struct DeviceParams {  // wl::WlParameters + the run_rewl intervals, on the devi
     int32_t inverse_time;
     int32_t nalivaiko;
     int32_t collect;
-    int32_t pad;
+    int32_t withhold_draws;  // failure injection: producers publish no draws (wlg_engine_inject_wait_timeout)
     double round_trip_margin;
     uint64_t exchange_interval;
     uint64_t max_attempts;     // 0 = unlimited

@@ -108,7 +108,69 @@ void* pool_allocate(size_t bytes) {
 }
 
 Engine::Engine(const wlg_system& system, const wlg_run_config& c) : cfg_(c) {
-    // RunConfig::validate (src/io.cpp:243-268), as run_rewl calls it.
+    configure(c);
+    validate_system(system);
+    check_backend(system.cutoff > 0.0);
+    // fingerprint of the system, so that a run checkpoint is never restored onto another one
+    {
+        uint64_t h = 1469598103934665603ULL;
+        auto mix = [&h](const void* p, size_t bytes) {
+            const unsigned char* c = static_cast<const unsigned char*>(p);
+            for (size_t k = 0; k < bytes; ++k) h = (h ^ c[k]) * 1099511628211ULL;
+        };
+        mix(system.positions, system.n * 24);
+        mix(system.axes, system.n * 24);
+        mix(system.box, sizeof system.box);
+        mix(&system.periodic, sizeof system.periodic);
+        mix(&system.coupling_scale, sizeof system.coupling_scale);
+        mix(&system.cutoff, sizeof system.cutoff);
+        system_hash_ = h;
+    }
+    require_device();
+    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    upload_system(system, sys_, stream_);
+    build_couplings(sys_, precision_, stream_);
+    initialise_walkers(c);
+}
+
+Engine::Engine(const wlg_couplings& couplings, const wlg_run_config& c) : cfg_(c) {
+    configure(c);
+    validate_couplings(couplings);
+    check_backend(couplings.dense == nullptr);
+    // fingerprint of the couplings (a different domain from the geometry fingerprint)
+    {
+        uint64_t h = 0x9e3779b97f4a7c15ULL;
+        auto mix = [&h](const void* p, size_t bytes) {
+            const unsigned char* c = static_cast<const unsigned char*>(p);
+            for (size_t k = 0; k < bytes; ++k) h = (h ^ c[k]) * 1099511628211ULL;
+        };
+        const uint64_t n = couplings.n;
+        mix(&n, sizeof n);
+        if (couplings.dense) {
+            mix(couplings.dense, n * n * 8);
+        } else {
+            mix(couplings.row_offsets, (n + 1) * 8);
+            mix(couplings.columns, couplings.nnz * 8);
+            mix(couplings.values, couplings.nnz * 8);
+        }
+        system_hash_ = h;
+    }
+    require_device();
+    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
+    check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+    upload_couplings(couplings, sys_, precision_, stream_);
+    initialise_walkers(c);
+}
+
+void Engine::check_backend(bool csr) const {
+    if (csr && precision_ == WLG_PRECISION_BF16)
+        throw WlgError(WLG_ERR_INVALID_ARGUMENT, "BF16 couplings are available for the dense backend only");
+}
+
+// The run configuration: RunConfig::validate (src/io.cpp:243-268), as run_rewl calls it, the
+// grid and windows, and the parameters the kernels read.
+void Engine::configure(const wlg_run_config& c) {
     if (!std::isfinite(c.progress_interval_seconds) || c.progress_interval_seconds < 0.0 || c.windows == 0 ||
         c.walkers_per_window == 0 || c.overlap < 0.0 || c.overlap >= 1.0 || c.exchange_interval_attempts == 0 ||
         c.wl.check_interval_attempts == 0 || c.checkpoint_interval_attempts == 0 ||
@@ -130,11 +192,8 @@ Engine::Engine(const wlg_system& system, const wlg_run_config& c) : cfg_(c) {
     } else {
         win_ = partition_windows(bins_, c.windows, c.overlap);
     }
-    validate_system(system);
     if (c.coupling_precision < WLG_PRECISION_FP64 || c.coupling_precision > WLG_PRECISION_BF16)
         throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Unknown coupling precision");
-    if (system.cutoff > 0.0 && c.coupling_precision == WLG_PRECISION_BF16)
-        throw WlgError(WLG_ERR_INVALID_ARGUMENT, "BF16 couplings are available for the dense backend only");
     if (c.windows * c.walkers_per_window > static_cast<uint64_t>(std::numeric_limits<int32_t>::max() / 64))
         throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Too many walkers");
     if (bins_ > static_cast<uint64_t>(std::numeric_limits<int32_t>::max() / 2))
@@ -164,28 +223,6 @@ Engine::Engine(const wlg_system& system, const wlg_run_config& c) : cfg_(c) {
     cfg_.initial_spins = nullptr;
     cfg_.initial_spins_present = nullptr;
     cfg_.checkpoint_path = nullptr;
-
-    // fingerprint of the system, so that a run checkpoint is never restored onto another one
-    {
-        uint64_t h = 1469598103934665603ULL;
-        auto mix = [&h](const void* p, size_t bytes) {
-            const unsigned char* c = static_cast<const unsigned char*>(p);
-            for (size_t k = 0; k < bytes; ++k) h = (h ^ c[k]) * 1099511628211ULL;
-        };
-        mix(system.positions, system.n * 24);
-        mix(system.axes, system.n * 24);
-        mix(system.box, sizeof system.box);
-        mix(&system.periodic, sizeof system.periodic);
-        mix(&system.coupling_scale, sizeof system.coupling_scale);
-        mix(&system.cutoff, sizeof system.cutoff);
-        system_hash_ = h;
-    }
-    require_device();
-    check_cuda(cudaGetDevice(&device), "cudaGetDevice");
-    check_cuda(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
-    upload_system(system, sys_, stream_);
-    build_couplings(sys_, precision_, stream_);
-    initialise_walkers(c);
 }
 
 Engine::~Engine() {
@@ -445,7 +482,19 @@ void Engine::check_device_error() {
     done_ = ctl.done != 0;
     epochs_ = ctl.epoch;
     if (ctl.error == WLG_ERR_ESCAPED) throw WlgError(WLG_ERR_ESCAPED, "Walker escaped its energy window");
+    if (ctl.error == WLG_ERR_TIMEOUT)
+        throw WlgError(WLG_ERR_TIMEOUT, "A bounded device wait gave up (walker " + std::to_string(ctl.error_walker) +
+                                            "); the walker's state was not written back");
     if (ctl.error) throw WlgError(static_cast<wlg_status>(ctl.error), "device error");
+}
+
+void Engine::inject_wait_timeout() {
+    view_.p.withhold_draws = 1;
+    // the epoch graph holds the kernels' arguments by value: capture it again
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    graph_exec_ = nullptr;
+    graph_ = nullptr;
 }
 
 void Engine::build_graph() {
@@ -1200,7 +1249,7 @@ void Engine::swap(uint64_t left, uint64_t right) {
 // ln f = 1): before the first attempt, every walker's window slice of log g is set from a
 // whole-grid estimate and its refinement factor to `factor`.  Bins outside the windows stay
 // zero, as in a fresh walker.
-void Engine::warm_start(const double* log_g, double factor) {
+void Engine::warm_start(const double* log_g, double factor, bool continue_schedule) {
     if (!log_g) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "null log g estimate");
     if (!std::isfinite(factor) || !(factor > 0.0))
         throw WlgError(WLG_ERR_INVALID_ARGUMENT, "The warm-start factor must be finite and positive");
@@ -1217,6 +1266,14 @@ void Engine::warm_start(const double* log_g, double factor) {
         for (uint64_t b = win_[2 * st.window]; b < win_[2 * st.window + 1]; ++b) grid[k * bins_ + b] = log_g[b];
         states[k].factor = factor;
         states[k].stage = factor <= p_.final_factor ? kFrozen : kWangLandau;
+        // continuing the 1/t schedule: the attempts a 1/t run over the window's bins would
+        // have made to reach ln f = factor count as made before the run
+        const double offset = continue_schedule
+                                  ? std::nearbyint(static_cast<double>(win_[2 * st.window + 1] - win_[2 * st.window]) / factor)
+                                  : 0.0;
+        if (!(offset < 0x1.0p62))
+            throw WlgError(WLG_ERR_INVALID_ARGUMENT, "The warm-start factor is too small to continue the 1/t schedule");
+        states[k].time_offset = static_cast<uint64_t>(offset);
     }
     check_cuda(cudaMemcpyAsync(d_log_g_.ptr, grid.data(), grid.size() * sizeof(double), cudaMemcpyHostToDevice,
                                stream_),

@@ -98,6 +98,10 @@ void validate_grid(double emin, double emax, double width);
 uint64_t grid_bins(double emin, double emax, double width);
 std::vector<uint64_t> partition_windows(uint64_t bins, uint64_t count, double overlap);
 void upload_system(const wlg_system& s, DeviceSystem& d, cudaStream_t stream);
+// Prebuilt couplings: validated (symmetric, zero diagonal, finite; CSR rows sorted by column)
+// and uploaded in the layouts build_couplings produces.
+void validate_couplings(const wlg_couplings& j);
+void upload_couplings(const wlg_couplings& j, DeviceSystem& d, int precision, cudaStream_t stream);
 void upload_cell_grid(const wlg_system& s, DeviceSystem& d, cudaStream_t stream);
 void save_checkpoint_file(const std::string& path, const wlg_snapshot& s, uint64_t n, uint64_t bins);
 bool load_checkpoint_file(const std::string& path, std::vector<int8_t>& spins, std::vector<double>& fields,
@@ -241,6 +245,8 @@ class Batch {
 class Engine {
   public:
     Engine(const wlg_system& system, const wlg_run_config& config);
+    // From prebuilt couplings (no geometry): the J a Couplings object exports.
+    Engine(const wlg_couplings& couplings, const wlg_run_config& config);
     ~Engine();
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
@@ -252,6 +258,9 @@ class Engine {
     void time_run(uint64_t epochs, wlg_epoch_timing* out);
     void autotune(uint64_t trial_epochs, wlg_autotune_report* out);
     void set_launch(int walkers_per_block, int epochs_per_graph);
+    // Failure injection for tests: from the next epoch on, the draw producers of the split and
+    // single-window sweeps publish nothing, so every walker's bounded wait runs out.
+    void inject_wait_timeout();
     uint64_t walkers() const { return walkers_; }
     uint64_t bins() const { return bins_; }
     uint64_t spins() const { return sys_.n; }
@@ -271,7 +280,10 @@ class Engine {
     double exchange_log_probability(uint64_t left, uint64_t right);
     void swap(uint64_t left, uint64_t right);
     void precision_report(wlg_precision_report* out);
-    void warm_start(const double* log_g, double factor);
+    // continue_schedule: each walker's 1/t stage counts window bins / factor attempts as made
+    // before the run (f = active / (attempted + offset)), so the factor never rises above the
+    // warm start's; false keeps the reference's rule (f = active / attempted).
+    void warm_start(const double* log_g, double factor, bool continue_schedule = false);
     // every walker's state, the control block and the recompute schedule (multi-walker
     // checkpoint; the reference checkpoints single-walker runs only)
     void save_run(const std::string& path);
@@ -294,6 +306,8 @@ class Engine {
     int device = 0;  // CUDA device the engine lives on
 
   private:
+    void configure(const wlg_run_config& c);
+    void check_backend(bool csr) const;
     void initialise_walkers(const wlg_run_config& c);
     void check_device_error();
     void launch_epochs(uint64_t count);

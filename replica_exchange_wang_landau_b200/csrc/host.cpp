@@ -1,7 +1,9 @@
 // host.cpp — host-side pieces that need no GPU: validation with the reference's messages,
 // the energy grid, the window partition, geometry upload and the WLCHKP checkpoint format.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <filesystem>
 #include <fstream>
 #include <limits>
@@ -35,6 +37,59 @@ void validate_system(const wlg_system& s) {
     }
     if (s.n > static_cast<uint64_t>(std::numeric_limits<int32_t>::max() / 2))
         throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Too many sites for one device system");
+}
+
+// Prebuilt couplings must be what the reference's backends produce: a symmetric matrix with
+// a zero diagonal and finite values (DenseCouplings fills both triangles with the same pair
+// value, src/physics.cpp:172-188; CsrCouplings stores every pair in both directions, sorted
+// by (row, column), src/physics.cpp:197-223).  The engine's sweeps read a row of J as the
+// column add_flip_delta reads, which is only the same thing for a symmetric J.
+void validate_couplings(const wlg_couplings& j) {
+    const uint64_t n = j.n;
+    if (n == 0) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Couplings contain no sites");
+    if (n > static_cast<uint64_t>(std::numeric_limits<int32_t>::max() / 2))
+        throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Too many sites for one device system");
+    if (j.dense) {
+        for (uint64_t r = 0; r < n; ++r) {
+            if (j.dense[r * n + r] != 0.0)
+                throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Couplings must have a zero diagonal");
+            for (uint64_t c = r + 1; c < n; ++c) {
+                const double a = j.dense[r * n + c], b = j.dense[c * n + r];
+                if (!std::isfinite(a)) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Couplings must be finite");
+                if (std::memcmp(&a, &b, sizeof a) != 0)
+                    throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Couplings must be symmetric");
+            }
+        }
+        return;
+    }
+    if (!j.row_offsets || (j.nnz > 0 && (!j.columns || !j.values)))
+        throw WlgError(WLG_ERR_INVALID_ARGUMENT, "CSR couplings need row offsets, columns and values");
+    if (j.row_offsets[0] != 0 || j.row_offsets[n] != j.nnz)
+        throw WlgError(WLG_ERR_INVALID_ARGUMENT, "CSR row offsets must start at 0 and end at nnz");
+    if (j.nnz > static_cast<uint64_t>(std::numeric_limits<int32_t>::max()))
+        throw WlgError(WLG_ERR_INVALID_ARGUMENT, "CSR has more than 2^31 couplings");
+    for (uint64_t r = 0; r < n; ++r) {
+        const uint64_t b = j.row_offsets[r], e = j.row_offsets[r + 1];
+        if (e < b || e > j.nnz) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "CSR row offsets must be non-decreasing");
+        for (uint64_t k = b; k < e; ++k) {
+            const uint64_t c = j.columns[k];
+            if (c >= n) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "CSR column out of range");
+            if (c == r) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Couplings must have a zero diagonal");
+            if (k > b && c <= j.columns[k - 1])
+                throw WlgError(WLG_ERR_INVALID_ARGUMENT, "CSR columns must ascend within a row");
+            if (!std::isfinite(j.values[k])) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Couplings must be finite");
+        }
+    }
+    for (uint64_t r = 0; r < n; ++r)
+        for (uint64_t k = j.row_offsets[r]; k < j.row_offsets[r + 1]; ++k) {
+            const uint64_t c = j.columns[k];
+            const uint64_t* first = j.columns + j.row_offsets[c];
+            const uint64_t* last = j.columns + j.row_offsets[c + 1];
+            const uint64_t* at = std::lower_bound(first, last, r);
+            if (at == last || *at != r ||
+                std::memcmp(&j.values[at - j.columns], &j.values[k], sizeof(double)) != 0)
+                throw WlgError(WLG_ERR_INVALID_ARGUMENT, "Couplings must be symmetric");
+        }
 }
 
 // EnergyGrid::validate (src/wang_landau.cpp:13-20)

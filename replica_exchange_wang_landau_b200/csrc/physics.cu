@@ -431,6 +431,80 @@ void launch_dense_build(const double* pos, const double* axes, const double* box
     check_cuda(cudaGetLastError(), "dense_build_kernel");
 }
 
+// The FP32 / BF16 (+ row scale) copies of a dense FP64 J.
+static void build_dense_lowp(DeviceSystem& d, int precision, cudaStream_t stream) {
+    if (precision == WLG_PRECISION_FP32) d.J32.allocate(d.ld * d.ld * sizeof(float));
+    if (precision == WLG_PRECISION_BF16) {
+        d.J16.allocate(d.ld * d.ld * sizeof(__nv_bfloat16));
+        d.Jscale.allocate(d.ld * sizeof(float));
+    }
+    if (precision != WLG_PRECISION_FP64) {
+        dense_lowp_kernel<<<static_cast<unsigned>(d.ld), 256, 0, stream>>>(
+            d.J64.get<double>(), static_cast<int>(d.n), static_cast<int>(d.ld), d.J32.get<float>(),
+            d.J16.get<__nv_bfloat16>(), d.Jscale.get<float>());
+        check_cuda(cudaGetLastError(), "dense_lowp_kernel");
+    }
+}
+
+// The ELLPACK copy read by the CSR sweep (rows of at most 256 couplings; zmax = longest row).
+static void build_ellpack(DeviceSystem& d, int precision, int32_t zmax, cudaStream_t stream) {
+    const int n = static_cast<int>(d.n);
+    int32_t width = 32;
+    while (width < zmax && width < 256) width *= 2;
+    if (zmax <= 256) {
+        const size_t entries = static_cast<size_t>(n) * static_cast<size_t>(width);
+        d.ell_col.allocate(entries * sizeof(int32_t));
+        if (precision == WLG_PRECISION_FP32) d.ell_val32.allocate(entries * sizeof(float));
+        else d.ell_val64.allocate(entries * sizeof(double));
+        launch_ell_fill(n, width, d.csr_ptr.get<int32_t>(), d.csr_col.get<int32_t>(), d.csr_val64.get<double>(),
+                        d.csr_val32.get<float>(), d.ell_col.get<int32_t>(), d.ell_val64.get<double>(),
+                        d.ell_val32.get<float>(), stream);
+        d.ell_width = width;
+    }
+}
+
+void upload_couplings(const wlg_couplings& j, DeviceSystem& d, int precision, cudaStream_t stream) {
+    d.n = j.n;
+    d.ld = (j.n + 15) / 16 * 16;
+    d.csr = j.dense == nullptr;
+    const uint64_t n = j.n;
+    if (!d.csr) {
+        d.J64.allocate(d.ld * d.ld * sizeof(double));
+        check_cuda(cudaMemsetAsync(d.J64.ptr, 0, d.J64.bytes, stream), "memset J");
+        check_cuda(cudaMemcpy2DAsync(d.J64.ptr, d.ld * sizeof(double), j.dense, n * sizeof(double), n * sizeof(double),
+                                     n, cudaMemcpyHostToDevice, stream),
+                   "copy J");
+        build_dense_lowp(d, precision, stream);
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+        return;
+    }
+    const size_t nnz = static_cast<size_t>(j.nnz);
+    std::vector<int32_t> ptr(n + 1), col(std::max<size_t>(1, nnz));
+    std::vector<float> v32;
+    int32_t zmax = 0;
+    for (uint64_t r = 0; r <= n; ++r) ptr[r] = static_cast<int32_t>(j.row_offsets[r]);
+    for (uint64_t r = 0; r < n; ++r) zmax = std::max(zmax, ptr[r + 1] - ptr[r]);
+    for (size_t k = 0; k < nnz; ++k) col[k] = static_cast<int32_t>(j.columns[k]);
+    d.nnz = nnz;
+    d.csr_ptr.allocate(ptr.size() * sizeof(int32_t));
+    d.csr_col.allocate(col.size() * sizeof(int32_t));
+    d.csr_val64.allocate(std::max<size_t>(1, nnz) * sizeof(double));
+    check_cuda(cudaMemcpyAsync(d.csr_ptr.ptr, ptr.data(), d.csr_ptr.bytes, cudaMemcpyHostToDevice, stream), "copy ptr");
+    check_cuda(cudaMemcpyAsync(d.csr_col.ptr, col.data(), nnz * sizeof(int32_t), cudaMemcpyHostToDevice, stream),
+               "copy columns");
+    check_cuda(cudaMemcpyAsync(d.csr_val64.ptr, j.values, nnz * sizeof(double), cudaMemcpyHostToDevice, stream),
+               "copy values");
+    if (precision == WLG_PRECISION_FP32) {
+        v32.resize(std::max<size_t>(1, nnz));
+        for (size_t k = 0; k < nnz; ++k) v32[k] = static_cast<float>(j.values[k]);  // as csr_fill_kernel rounds
+        d.csr_val32.allocate(v32.size() * sizeof(float));
+        check_cuda(cudaMemcpyAsync(d.csr_val32.ptr, v32.data(), nnz * sizeof(float), cudaMemcpyHostToDevice, stream),
+                   "copy values");
+    }
+    build_ellpack(d, precision, zmax, stream);
+    check_cuda(cudaStreamSynchronize(stream), "sync");
+}
+
 void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream) {
     const SystemView s = make_view(d);
     DeviceBuffer err(sizeof(int));
@@ -443,17 +517,7 @@ void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream) {
         dense_build_kernel<<<dim3(tiles, tiles), dim3(32, 8), 0, stream>>>(s, static_cast<int>(d.ld),
                                                                            d.J64.get<double>(), err.get<int>());
         check_cuda(cudaGetLastError(), "dense_build_kernel");
-        if (precision == WLG_PRECISION_FP32) d.J32.allocate(d.ld * d.ld * sizeof(float));
-        if (precision == WLG_PRECISION_BF16) {
-            d.J16.allocate(d.ld * d.ld * sizeof(__nv_bfloat16));
-            d.Jscale.allocate(d.ld * sizeof(float));
-        }
-        if (precision != WLG_PRECISION_FP64) {
-            dense_lowp_kernel<<<static_cast<unsigned>(d.ld), 256, 0, stream>>>(
-                d.J64.get<double>(), n, static_cast<int>(d.ld), d.J32.get<float>(), d.J16.get<__nv_bfloat16>(),
-                d.Jscale.get<float>());
-            check_cuda(cudaGetLastError(), "dense_lowp_kernel");
-        }
+        build_dense_lowp(d, precision, stream);
     } else {
         DeviceBuffer counts(static_cast<size_t>(n) * sizeof(int32_t));
         const int warps_per_block = 8;
@@ -497,21 +561,9 @@ void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream) {
                                                                       d.csr_val64.get<double>(), d.csr_val32.get<float>());
             check_cuda(cudaGetLastError(), "csr_scan_fill_kernel");
         }
-        // the ELLPACK copy read by the CSR sweep (rows of at most 256 couplings)
         int32_t zmax = 0;
         for (int32_t c : host_counts) zmax = std::max(zmax, c);
-        int32_t width = 32;
-        while (width < zmax && width < 256) width *= 2;
-        if (zmax <= 256) {
-            const size_t entries = static_cast<size_t>(n) * static_cast<size_t>(width);
-            d.ell_col.allocate(entries * sizeof(int32_t));
-            if (precision == WLG_PRECISION_FP32) d.ell_val32.allocate(entries * sizeof(float));
-            else d.ell_val64.allocate(entries * sizeof(double));
-            launch_ell_fill(n, width, d.csr_ptr.get<int32_t>(), d.csr_col.get<int32_t>(), d.csr_val64.get<double>(),
-                            d.csr_val32.get<float>(), d.ell_col.get<int32_t>(), d.ell_val64.get<double>(),
-                            d.ell_val32.get<float>(), stream);
-            d.ell_width = width;
-        }
+        build_ellpack(d, precision, zmax, stream);
     }
     int host_err = 0;
     check_cuda(cudaMemcpyAsync(&host_err, err.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream), "copy err");

@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_kernel(EngineView v, WalkAr
         }
         ++t;
         if (stage == kInverseTime) {  // update_inverse_time_factor
-            factor = inverse_time_factor(itt, att0 + t - 1, active_count, factor, lane);
+            factor = inverse_time_factor(itt, att0 + st.time_offset + t - 1, active_count, factor, lane);
             if (factor <= P.final_factor) stage = kFrozen;
         }
         if (accepted && nb != cur) {  // update_current_bin moves to the new bin
@@ -661,7 +661,8 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
                                                     : reinterpret_cast<const JT*>(v.J16);
         Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};
         uint32_t produced = 0, status = 0;
-        for (;;) {
+        // withhold_draws: publish nothing, so that the walker's bounded wait runs out
+        for (bool open = P.withhold_draws == 0; open;) {
             uint32_t consumed = __shfl_sync(kFull, lane == 0 ? ld_acquire_shared(consumed_addr) : 0u, 0);
             if (produced + kDrawBatch - consumed > qm + 1) {  // no room for a batch yet
                 uint32_t go = 0;
@@ -880,7 +881,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
 
             // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
             if (kIT && stage == kInverseTime) {  // resolved at the next read of log g
-                f_p = inverse_time_factor(itt, att0 + t - 1, active_count, factor, lane);
+                f_p = inverse_time_factor(itt, att0 + st.time_offset + t - 1, active_count, factor, lane);
                 pend = true;
             }
             const bool move = accepted && nb != cur;

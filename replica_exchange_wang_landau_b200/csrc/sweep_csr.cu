@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(256, 1) sweep_csr_kernel(EngineView v, WalkArg
 
             // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
             if (kIT && stage == kInverseTime) {  // resolved at the next read of log g
-                f_p = inverse_time_factor(itt, att0 + t - 1, active_count, factor, lane);
+                f_p = inverse_time_factor(itt, att0 + st.time_offset + t - 1, active_count, factor, lane);
                 pend = true;
             }
             const bool move = accepted && nb != cur;

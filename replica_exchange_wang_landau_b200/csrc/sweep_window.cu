@@ -141,7 +141,8 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
         const FastMod fm = v.site_mod;
         Rng rng{st.rng[0], st.rng[1], st.rng[2], st.rng[3]};
         uint32_t produced = 0, timeout = 0;
-        for (;;) {
+        // withhold_draws: publish nothing, so that the walkers' bounded waits run out
+        for (bool open = v.p.withhold_draws == 0; open;) {
             uint32_t go = 0;
             if (lane == 0) {
                 for (uint32_t polls = 0; polls < kWindowProducerPolls; ++polls) {
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
 
                     // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
                     if (kIT && stage == kInverseTime) {  // resolved at the next read of log g
-                        f_p = inverse_time_factor(itt, att0 + t - 1, active_count, factor, lane);
+                        f_p = inverse_time_factor(itt, att0 + st.time_offset + t - 1, active_count, factor, lane);
                         pend = true;
                     }
                     const bool move = accepted && nb != cur;

@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(256) walk_kernel(EngineView v, WalkArgs a) {
         }
         if (stage == kInverseTime) {  // update_inverse_time_factor
             if (active_count != 0 && att != 0)
-                factor = static_cast<double>(active_count) / static_cast<double>(att);
+                factor = static_cast<double>(active_count) / static_cast<double>(att + st.time_offset);
             if (factor <= P.final_factor) stage = kFrozen;
         }
         // update_current_bin

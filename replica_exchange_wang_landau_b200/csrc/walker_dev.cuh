@@ -107,9 +107,9 @@ __device__ __forceinline__ void warp_begin_next_iteration(WalkerState& st, uint6
         st.refine_count = 0;
     }
     if (p.inverse_time) {
-        const double inverse_time = st.attempted == 0
-                                        ? 1.0
-                                        : static_cast<double>(st.active_count) / static_cast<double>(st.attempted);
+        const double inverse_time =
+            st.attempted == 0 ? 1.0
+                              : static_cast<double>(st.active_count) / static_cast<double>(st.attempted + st.time_offset);
         if (st.factor <= inverse_time) {
             st.stage = kInverseTime;
             st.factor = inverse_time;
@@ -120,7 +120,8 @@ __device__ __forceinline__ void warp_begin_next_iteration(WalkerState& st, uint6
 }
 
 // update_inverse_time_factor (src/wang_landau.cpp:300-315) for consecutive attempts of the 1/t
-// stage: f = active_bins / attempted, the attempted count including the attempt.  An IEEE
+// stage: f = active_bins / attempted, the attempted count including the attempt (plus the
+// walker's time_offset, 0 unless a warm start continues the schedule).  An IEEE
 // division is a dependent sequence of about 170 cycles that the warp would otherwise wait for
 // on every attempt; here lane j divides for the j-th attempt of a block of 32 (the same
 // operands, so the same quotient), and an attempt takes its quotient by a shuffle.  A block

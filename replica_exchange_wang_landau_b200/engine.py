@@ -227,6 +227,58 @@ class System:
         return (fields[0], energies[0]) if single else (fields, energies)
 
 
+class Couplings:
+    """Prebuilt couplings as wl::Couplings::at(i, j) exports them (include/wl/physics.hpp:41-49):
+    a dense (n, n) matrix, or CSR rows (row_offsets, columns, values) sorted by column.  An
+    Engine built from them runs exactly as one built from the geometry they came from."""
+
+    def __init__(self, dense: Optional[np.ndarray] = None, row_offsets=None, columns=None, values=None):
+        if (dense is None) == (row_offsets is None):
+            raise InvalidArgument(1, "give either a dense matrix or CSR rows")
+        if dense is not None:
+            self.dense = np.ascontiguousarray(dense, dtype=np.float64)
+            if self.dense.ndim != 2 or self.dense.shape[0] != self.dense.shape[1]:
+                raise InvalidArgument(1, "dense couplings must be a square matrix")
+            self.n = int(self.dense.shape[0])
+        else:
+            self.dense = None
+            self.row_offsets = np.ascontiguousarray(row_offsets, dtype=np.uint64)
+            self.columns = np.ascontiguousarray(columns, dtype=np.uint64)
+            self.values = np.ascontiguousarray(values, dtype=np.float64)
+            self.n = int(self.row_offsets.shape[0]) - 1
+            if self.columns.shape != self.values.shape:
+                raise InvalidArgument(1, "CSR columns and values differ in length")
+
+    @staticmethod
+    def of(system: "System") -> "Couplings":
+        """The couplings the reference's backend for `system` stores (dense or CSR)."""
+        if system.backend == "csr":
+            ptr, cols, vals = system.csr()
+            return Couplings(row_offsets=ptr, columns=cols, values=vals)
+        return Couplings(dense=system.couplings("fp64"))
+
+    @property
+    def backend(self) -> str:
+        return "dense" if self.dense is not None else "csr"
+
+    def size(self) -> int:
+        return self.n
+
+    def _struct(self) -> _abi.wlg_couplings:
+        c = _abi.wlg_couplings()
+        c.n = self.n
+        if self.dense is not None:
+            c.dense = _dptr(self.dense)
+            c._keep = (self.dense,)
+        else:
+            c.nnz = int(self.columns.shape[0])
+            c.row_offsets = _u64ptr(self.row_offsets)
+            c.columns = _u64ptr(self.columns)
+            c.values = _dptr(self.values)
+            c._keep = (self.row_offsets, self.columns, self.values)
+        return c
+
+
 # ---- configuration -------------------------------------------------------------------
 
 
@@ -492,7 +544,8 @@ def _stat_dict(s: _abi.wlg_walker_statistics) -> dict:
 class Engine:
     """One REWL run resident on the current CUDA device (run_rewl's state, src/parallel.cpp:276-534)."""
 
-    def __init__(self, system: System, config: RunConfig, walkers_per_block: int | None = None):
+    def __init__(self, system: "System | Couplings", config: RunConfig, walkers_per_block: int | None = None):
+        """`system` is a System (geometry: J is built on the device) or prebuilt Couplings."""
         self._lib = load_library()
         self.system = system
         self.config = config
@@ -500,7 +553,9 @@ class Engine:
         self._sys = system._struct()
         self._cfg, self._keep = config._struct(n)
         handle = C.c_void_p()
-        _check(self._lib.wlg_engine_create(C.byref(self._sys), C.byref(self._cfg), C.byref(handle)))
+        create = self._lib.wlg_engine_create_from_couplings if isinstance(system, Couplings) else \
+            self._lib.wlg_engine_create
+        _check(create(C.byref(self._sys), C.byref(self._cfg), C.byref(handle)))
         self._h = handle
         self.n = n
         self.bins = int(self._lib.wlg_engine_bins(self._h))
@@ -572,13 +627,22 @@ class Engine:
         out["coupling_precision"] = {v: k for k, v in _abi.PRECISION.items()}[r.coupling_precision]
         return out
 
-    def warm_start(self, log_g: np.ndarray, factor: float) -> None:
+    def warm_start(self, log_g: np.ndarray, factor: float, continue_schedule: bool = False) -> None:
         """Seeds every walker's window slice of log g (whole-grid array) and its ln f before
-        the first attempt (no counterpart in the reference)."""
+        the first attempt (no counterpart in the reference).  continue_schedule: the 1/t
+        stage continues from ln f = factor (f = active / (attempted + window bins / factor))
+        instead of restarting at active / attempted."""
         lg = np.ascontiguousarray(log_g, dtype=np.float64)
         if lg.shape != (self.bins,):
             raise InvalidArgument(1, "The log g estimate must have one entry per grid bin")
-        _check(self._lib.wlg_engine_warm_start(self._h, _dptr(lg), float(factor)))
+        fn = self._lib.wlg_engine_warm_start_continue if continue_schedule else self._lib.wlg_engine_warm_start
+        _check(fn(self._h, _dptr(lg), float(factor)))
+
+    def inject_wait_timeout(self) -> None:
+        """Failure injection for tests: the draw producers of the split and single-window sweeps
+        publish nothing from the next epoch on, so the walkers' bounded waits run out and the
+        next run call raises a DeviceError with status WLG_ERR_TIMEOUT."""
+        _check(self._lib.wlg_engine_inject_wait_timeout(self._h))
 
     def set_launch(self, walkers_per_block: int = 0, epochs_per_graph: int = 0) -> None:
         _check(self._lib.wlg_engine_set_launch(self._h, int(walkers_per_block), int(epochs_per_graph)))

@@ -12,6 +12,8 @@ int main(void) {
     printf("{");
     S(wlg_system); F(wlg_system, n); F(wlg_system, positions); F(wlg_system, axes); F(wlg_system, box);
     F(wlg_system, periodic); F(wlg_system, coupling_scale); F(wlg_system, cutoff);
+    S(wlg_couplings); F(wlg_couplings, n); F(wlg_couplings, dense); F(wlg_couplings, nnz);
+    F(wlg_couplings, row_offsets); F(wlg_couplings, columns); F(wlg_couplings, values);
     S(wlg_wl_parameters); F(wlg_wl_parameters, flatness); F(wlg_wl_parameters, minimum_visits);
     F(wlg_wl_parameters, final_factor); F(wlg_wl_parameters, check_interval_attempts);
     F(wlg_wl_parameters, force_accept_after_attempts); F(wlg_wl_parameters, inverse_time_enabled);
