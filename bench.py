@@ -315,7 +315,7 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
                 except Exception as exc:
                     line["time_to_converge"] = {"error": str(exc)}
             try:
-                line["time_to_accuracy"] = time_to_accuracy()
+                line["time_to_accuracy"] = learned_configuration_line()
             except Exception as exc:
                 line["time_to_accuracy"] = {"error": str(exc)}
         print(json.dumps(line))
@@ -370,13 +370,20 @@ def mixed_precision_lines(epochs: int = 10) -> dict:
     from replica_exchange_wang_landau_b200.engine import Engine
     out = {}
     system, configs = mixed_precision_workload()
-    for precision, config in configs.items():
+    frags = {}
+    for precision, config in [*configs.items(), ("fp64_seed2", None)]:
+        if config is None:  # the FP64 run with another seed: the sampling noise of log g
+            config = copy.deepcopy(configs["fp64"])
+            config.seed = 2
         t0 = time.perf_counter()
         with Engine(system, config) as eng:
             create_s = time.perf_counter() - t0
             eng.time_run(2)
             t = eng.time_run(epochs)
             rep = eng.precision_report()
+            frags[precision] = (eng.fragments(allow_empty=True), [st["energy"] for st in eng.walker_statistics()])
+        if precision == "fp64_seed2":
+            continue
         out[precision] = {"value": t["attempted"] / (t["total_ms"] / 1e3), "unit": UNIT, "epochs_timed": t["epochs"],
                           "ms_per_epoch": t["total_ms"] / max(1, t["epochs"]),
                           "recompute_interval_mcs": 1.0 if precision != "fp64" else None,
@@ -384,6 +391,25 @@ def mixed_precision_lines(epochs: int = 10) -> dict:
                           "max_energy_drift": rep["max_energy_drift"], "deferred": rep["deferred"],
                           "bin_changes": rep["bin_changes"], "engine_create_s": create_s,
                           "acceptance": t["accepted"] / max(1, t["attempted"])}
+    # log g of each form against the FP64 run with the same seed after the same epochs: per window,
+    # max |d - mean(d)| over the bins valid in both; the FP64 run with another seed gives the
+    # sampling noise at this point of the run.  With the same seed a narrow-J walker follows the
+    # FP64 walker draw for draw until an accumulated field error first changes a decision (a
+    # bin), so "same_trajectory" counts the walkers whose energy is still the FP64 walker's.
+    base, base_e = frags["fp64"]
+    for name in ("fp32", "bf16", "fp64_seed2"):
+        if name not in frags:
+            continue
+        worst = 0.0
+        for fa, fb in zip(frags[name][0], base):
+            ok = (fa.valid == 1) & (fb.valid == 1)
+            if ok.sum() >= 2:
+                d = fa.log_g[ok] - fb.log_g[ok]
+                worst = max(worst, float(np.max(np.abs(d - d.mean()))))
+        same = sum(1 for a, b in zip(frags[name][1], base_e) if float(a).hex() == float(b).hex())
+        key = name if name in out else "fp64_other_seed"
+        out.setdefault(key, {}).update({"max_abs_dlog_g_vs_fp64": worst, "same_trajectory_walkers": same,
+                                        "walkers": len(base_e), "after_epochs": epochs + 2})
     out["workload"] = ("16x16x16 simple cubic, 40% of sites removed (seed 1, N = 2458), slab box (16, 16, 0), "
                        "random-sphere axes, dense J; 32 windows x 8 walkers, exchange and FP64 recompute every MCS; "
                        f"grid [{config.emin:g}, {config.emax:g}] in bins of {config.bin_width:g}")
@@ -516,68 +542,147 @@ def csr_batched_line(epochs: int = 40, pilot_mcs: float = 20.0, with_cpu_baselin
             "max_field_drift": rep["max_field_drift"]}
 
 
-def _cluster(k: int):
-    from replica_exchange_wang_landau_b200.engine import System
-    from replica_exchange_wang_landau_b200.geometry import random_sequential
-    rng = np.random.default_rng(k)
-    n = int(rng.integers(8, 13))
-    return System(random_sequential(n, float(rng.uniform(0.3, 0.8)), 0.8, seed=k), 1.0, 0.0)
-
-
-def _enumerate(system):
-    """Exact log g of a small system by enumerating its 2^N configurations (numpy), on a grid
-    of about 64 power-of-two bins padded by one bin."""
-    import itertools
-    import math
-    n = system.size()
-    j = system.couplings("fp64")[:n, :n]
-    states = np.array(list(itertools.product([-1.0, 1.0], repeat=n)))
-    e = 0.5 * np.einsum("ki,ij,kj->k", states, j, states)
-    w = 2.0 ** round(math.log2((e.max() - e.min()) / 64))
-    emin, emax = math.floor(e.min() / w) * w - w, math.ceil(e.max() / w) * w + w
-    counts = np.bincount(np.floor((e - emin) / w).astype(int), minlength=int(round((emax - emin) / w)))
-    ref = np.where(counts > 0, np.log(np.maximum(counts, 1).astype(float)), np.nan)
-    return emin, emax, w, ref
-
-
-def time_to_accuracy(tolerance: float = 0.05, held_out: int = 24) -> dict:
-    """Learned vs plain: the warm-start network is trained on the GPU on 48 plain-run DOS
-    curves of random dipole clusters (8-12 spins, density 0.3-0.8, random axes); each of
-    `held_out` other clusters is then run from the flat start and from the learned start (ln f =
-    1e-2) until max |d log g| against exact enumeration is <= tolerance."""
-    from replica_exchange_wang_landau_b200.warmstart import WarmStartModel, plain_dos_many, run_to_accuracy
+def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e-3, judge_factor: float = 3e-6,
+                               sequential_sample: int = 8, cpu_sample: int = 2) -> dict:
+    """The learned configuration, time to accuracy: 256 generated dilute systems (N uniform in
+    64..1024, random sequential addition at density 0.3-0.8, random-sphere axes; one window of 2
+    walkers over about +-4 sigma in 200 bins).  The warm-start network is trained on the GPU on
+    plain-run DOS curves (ln f = 1e-4) of the first 200; the other 56 are held out.  Each held-out
+    system's judge is a long plain FP64 run of its own (flat start, other seeds, ln f =
+    judge_factor).  Time until max |d log g| <= tolerance against the judge, for:
+      plain_sequential -- the plain FP64 GPU form: flat start, one engine at a time (measured on
+                          `sequential_sample` systems, the total for 56 scaled from their mean);
+      plain_batched    -- the same engines advanced together in one batch;
+      learned_batched  -- batched, FP64, learned warm start at ln f = start_factor continuing
+                          the 1/t schedule;
+      combined         -- batched, FP32 couplings with an FP64 recompute every epoch, learned
+                          warm start (the batched + mixed-precision + learned form).
+    Time to ln f <= 1e-8 of each arm is extrapolated from its measured attempts per walker per
+    second (1/t: active bins / 1e-8 attempts per walker, less the continued schedule's offset).
+    The reference's run_rewl (compiled from its sources, 2 walkers on 2 host threads) is timed
+    on `cpu_sample` held-out systems; its time to the tolerance is the plain runs' attempts per
+    walker over its rate, 56 systems on all host cores."""
+    from replica_exchange_wang_landau_b200.engine import Engine
+    from replica_exchange_wang_landau_b200.warmstart import (WarmStartModel, batch_to_accuracy, dilute_instance,
+                                                             engine_to_accuracy, plain_dos_many, single_window_config)
     t0 = time.perf_counter()
-    specs = []
-    for k in range(1, 49):
-        s = _cluster(k)
-        emin, emax, w, _ = _enumerate(s)
-        specs.append((s, emin, emax, w, k))
-    train = plain_dos_many(specs, final_factor=1e-4)  # the 48 plain runs side by side in one batch
+    systems = [dilute_instance(k) for k in range(256)]
+    setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    train = plain_dos_many([(s, lo, hi, w, k + 1) for k, (s, lo, hi, w) in enumerate(systems[:200])], final_factor=1e-4)
+    curves_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
     model = WarmStartModel(hidden=(32, 32), seed=3)
     loss = model.fit(train, steps=4000, learning_rate=3e-3)
-    train_s = time.perf_counter() - t0
-    rows = []
-    for k in range(1001, 1001 + held_out):
-        s = _cluster(k)
-        emin, emax, w, ref = _enumerate(s)
-        a = run_to_accuracy(s, emin, emax, w, ref, tolerance, seed=k)
-        b = run_to_accuracy(s, emin, emax, w, ref, tolerance, seed=k, model=model, factor=1e-2)
-        rows.append({"spins": s.size(), "plain_attempts": a["attempts"], "plain_s": a["seconds"],
-                     "learned_attempts": b["attempts"], "learned_s": b["seconds"]})
-    ok = [r for r in rows if r["plain_attempts"] and r["learned_attempts"]]
-    pa = sum(r["plain_attempts"] for r in ok)
-    la = sum(r["learned_attempts"] for r in ok)
-    ps = sum(r["plain_s"] for r in ok)
-    ls = sum(r["learned_s"] for r in ok)
-    ratios = sorted(r["learned_attempts"] / r["plain_attempts"] for r in ok)
-    return {"tolerance": tolerance, "criterion": "max |d log g| vs exact enumeration, 1 window x 2 walkers, 1/t",
-            "training": {"curves": len(train), "final_loss": loss, "seconds": train_s},
-            "held_out_systems": len(rows), "reached_tolerance": len(ok),
-            "plain_attempts_per_walker": pa, "learned_attempts_per_walker": la,
-            "plain_seconds": ps, "learned_seconds": ls, "attempts_ratio": la / pa if pa else None,
-            "seconds_ratio": ls / ps if ps else None,
-            "per_system_attempts_ratio": {"min": ratios[0], "median": ratios[len(ratios) // 2], "max": ratios[-1]}
-            if ratios else None}
+    fit_s = time.perf_counter() - t0
+    held = systems[200:]
+    t0 = time.perf_counter()
+    judged = plain_dos_many([(s, lo, hi, w, 10_000 + k) for k, (s, lo, hi, w) in enumerate(held)],
+                            final_factor=judge_factor)
+    judge_s = time.perf_counter() - t0
+    judges = [np.where(d.valid, d.log_g, np.nan) for d in judged]
+    # the learned prior's own error, before any sampling
+    prior_err = []
+    for (s, lo, hi, w), judge in zip(held, judges):
+        lg = model.predict_log_g(s, lo, hi, w)
+        prior_err.append(float(np.max(np.abs((lg - judge)[np.isfinite(judge)] -
+                                             np.nanmean(lg[np.isfinite(judge)] - judge[np.isfinite(judge)])))))
+
+    def engines(precision: str, learned: bool) -> list:
+        out = []
+        for k, (s, lo, hi, w) in enumerate(held):
+            e = Engine(s, single_window_config(lo, hi, w, s.size(), 20_000 + k, 1e-8, precision=precision))
+            if learned:
+                lg = model.predict_log_g(s, lo, hi, w)
+                e.warm_start(lg - lg.max(), start_factor, continue_schedule=True)
+            out.append(e)
+        return out
+
+    def to_ln_f_1e8(engs, rates) -> float:
+        # the batch runs every system at once: the slowest one sets the time (the continued
+        # schedule's offset, window bins / 1e-3, is 1e-5 of active / 1e-8 and is left out)
+        need = [float(np.mean([x["active_bins"] for x in e.walker_statistics()])) / 1e-8 for e in engs]
+        return max(n / r for n, r in zip(need, rates))
+
+    arms = {}
+    for name, precision, learned in (("plain_batched", "fp64", False), ("learned_batched", "fp64", True),
+                                     ("combined", "fp32", True)):
+        engs = engines(precision, learned)
+        try:
+            r = batch_to_accuracy(engs, judges, tolerance)
+            r["ln_f_1e-8_s_extrapolated"] = to_ln_f_1e8(engs, r["attempts_per_walker_per_s"])
+            if precision != "fp64":
+                reps = [e.precision_report() for e in engs]
+                r["max_field_drift"] = max(x["max_field_drift"] for x in reps)
+                r["bin_changes"] = sum(x["bin_changes"] for x in reps)
+        finally:
+            for e in engs:
+                e.close()
+        hits = [h for h in r["hit_attempts_per_walker"] if h is not None]
+        arms[name] = {"seconds_all": r["all_seconds"], "reached": r["reached"],
+                      "median_attempts_per_walker": float(np.median(hits)) if hits else None,
+                      "median_hit_seconds": float(np.median([h for h in r["hit_seconds"] if h is not None]))
+                      if hits else None,
+                      "max_final_error": max(r["final_errors"]),
+                      "ln_f_1e-8_s_extrapolated": r["ln_f_1e-8_s_extrapolated"],
+                      **({k: r[k] for k in ("max_field_drift", "bin_changes") if k in r})}
+    seq = []
+    for k in range(sequential_sample):
+        s, lo, hi, w = held[k]
+        with Engine(s, single_window_config(lo, hi, w, s.size(), 20_000 + k, 1e-8)) as e:
+            r = engine_to_accuracy(e, judges[k], tolerance)
+            active = float(np.mean([x["active_bins"] for x in e.walker_statistics()]))
+        r["ln_f_1e-8_s"] = active / 1e-8 / r["attempts_per_walker_per_s"]
+        r["active_bins"] = active
+        seq.append(r)
+    ok = [r for r in seq if r["seconds"] is not None]
+    per_system = float(np.mean([r["seconds"] for r in ok])) if ok else None
+    arms["plain_sequential"] = {
+        "systems_timed": len(seq), "reached": len(ok), "mean_seconds_per_system": per_system,
+        "seconds_all_56_scaled": per_system * len(held) if per_system else None,
+        "median_attempts_per_walker": float(np.median([r["attempts_per_walker"] for r in ok])) if ok else None,
+        "ln_f_1e-8_s_extrapolated_all_56": float(np.mean([r["ln_f_1e-8_s"] for r in seq])) * len(held)}
+    # the reference on the host: its rate on held-out systems, applied to the plain attempts
+    cpu = None
+    try:
+        from oracle.oracle import Reference
+        ref = Reference()
+        threads = ref.set_threads(2)
+        rates = []
+        for k in range(cpu_sample):
+            s, lo, hi, w = held[k]
+            c = single_window_config(lo, hi, w, s.size(), 20_000 + k, 1e-8)
+            c.max_mcs = 2000.0
+            c.resolved_spin_count = 0
+            c.resolve_mcs(s.size())
+            t1 = time.perf_counter()
+            rr = ref.run_rewl(s, c)
+            rates.append(rr.attempted / 2 / (time.perf_counter() - t1))
+        rate = float(np.mean(rates))
+        need = arms["plain_sequential"]["median_attempts_per_walker"]
+        parallel = max(1, (os.cpu_count() or 2) // 2)
+        cpu = {"attempts_per_walker_per_s": rate, "threads_per_system": threads, "systems_in_parallel": parallel,
+               "seconds_all_56_extrapolated": need / rate * len(held) / parallel if need else None,
+               "ln_f_1e-8_s_all_56_extrapolated": float(np.mean([r["active_bins"] for r in seq])) / 1e-8 / rate *
+               len(held) / parallel,
+               "sample": f"reference run_rewl (oracle/_ref) on {cpu_sample} held-out systems, 2 walkers on "
+                         f"{threads} threads, 2000 MCS"}
+    except Exception as exc:
+        cpu = {"error": str(exc)}
+    comb = arms["combined"]["seconds_all"]
+    seq_all = arms["plain_sequential"]["seconds_all_56_scaled"]
+    out = {"tolerance": tolerance, "criterion": "max |d log g - mean| against the system's own long plain FP64 run",
+           "systems": 256, "trained_on": 200, "held_out": len(held), "start_factor": start_factor,
+           "judge_final_factor": judge_factor,
+           "training": {"curves": len(train), "final_loss": loss, "curve_seconds": curves_s, "fit_seconds": fit_s},
+           "setup_s": setup_s, "judge_s": judge_s,
+           "prior_error": {"median": float(np.median(prior_err)), "max": float(np.max(prior_err))},
+           "arms": arms, "reference_cpu": cpu,
+           "combined_over_plain_sequential": seq_all / comb if (seq_all and comb) else None,
+           "combined_over_plain_batched": (arms["plain_batched"]["seconds_all"] / comb)
+           if (comb and arms["plain_batched"]["seconds_all"]) else None}
+    out["target_10x_met"] = bool(out["combined_over_plain_sequential"] and out["combined_over_plain_sequential"] >= 10)
+    return out
 
 
 def c1_config():
@@ -726,9 +831,14 @@ def main() -> None:
                     help="print only the mixed-precision configuration's lines (N = 2458, FP64 / FP32 / BF16)")
     ap.add_argument("--csr-only", action="store_true",
                     help="print only the CSR configuration's line (the 32^3 lattice, 1024 walkers)")
+    ap.add_argument("--learned-only", action="store_true",
+                    help="print only the learned configuration's time to accuracy (256 dilute systems)")
     args = ap.parse_args()
     if args.csr_only:
         print(json.dumps({"csr_batched": csr_batched_line()}))
+        return
+    if args.learned_only:
+        print(json.dumps({"time_to_accuracy": learned_configuration_line()}))
         return
     if args.batched_only:
         print(json.dumps({"batched_instances": batched_instances_line()}))

@@ -352,14 +352,15 @@ wlg_status wlg_engine_precision_report(wlg_engine* engine, wlg_precision_report*
  * reference, whose walkers start from log g = 0 and ln f = 1; the learned warm start
  * (replica_exchange_wang_landau_b200/warmstart.py) supplies the estimate. */
 wlg_status wlg_engine_warm_start(wlg_engine* engine, const double* log_g, double factor);
-/* The same warm start, continuing the 1/t schedule instead of restarting it: each walker counts
- * round(window bins / factor) attempts as already made, so that in the 1/t stage its factor is
- * f = active / (attempted + offset) (update_inverse_time_factor and begin_next_iteration,
- * src/wang_landau.cpp:309-315, 389-409, with the offset added to attempted).  Under the
- * reference's rule (offset 0) the first check after a warm start at a small ln f switches to
- * 1/t with f = active / attempted, far above the start's factor early in a run, which discards
- * the warm start; with the offset f starts at the warm start's factor and falls as 1/t from
- * there.  An extension with no counterpart in the reference. */
+/* The same warm start, continuing the 1/t schedule instead of restarting it.  Under the
+ * reference's rule (begin_next_iteration, src/wang_landau.cpp:389-409) the first covered check
+ * after a warm start at a small ln f switches to 1/t with f = active / attempted, far above the
+ * start's factor early in a run, which discards the warm start.  Here that check halves ln f as
+ * usual and then enters the 1/t stage at once from the factor reached, counting
+ * round(active / factor) - attempted attempts as already made: from then on
+ * f = active / (attempted + offset) (update_inverse_time_factor, src/wang_landau.cpp:309-315,
+ * with the offset added), so f never rises above the warm start's and falls as 1/t.  An
+ * extension with no counterpart in the reference. */
 wlg_status wlg_engine_warm_start_continue(wlg_engine* engine, const double* log_g, double factor);
 uint64_t wlg_engine_walkers(const wlg_engine* engine);
 uint64_t wlg_engine_bins(const wlg_engine* engine);
@@ -437,6 +438,18 @@ wlg_status wlg_stitch_dos(double emin, double emax, double width, const wlg_frag
                           uint64_t count, int32_t complete_range, uint64_t spin_count, double* log_g,
                           uint64_t* histogram, double* standard_error, uint8_t* valid, wlg_join_quality* joins,
                           int32_t* fully_normalized);
+/* The engine's stitched density of states: stitch_dos (src/analysis.cpp:45-130) of every
+ * window's fragment, computed on the device from the fragments summarize leaves there, bit
+ * for bit the curve wlg_stitch_dos gives (and the reference's stitch_dos) for the same
+ * fragments.  Arrays hold grid-bins entries; joins holds windows - 1 entries (or NULL);
+ * complete_range normalises sum g = 2^N (the one exp / log sum of that step runs on the host,
+ * with the C library the reference uses), else the peak is 0.  The reference's errors, with
+ * its messages: a window whose walkers share no active bin, adjacent fragments without a
+ * common valid bin, complete_range with an invalid bin, no valid bin at all.  No counterpart
+ * in the reference, which stitches on the host after run_rewl returns (apps/wl_run.cpp:180). */
+wlg_status wlg_engine_stitch(wlg_engine* engine, int32_t complete_range, double* log_g, uint64_t* histogram,
+                             double* standard_error, uint8_t* valid, wlg_join_quality* joins,
+                             int32_t* fully_normalized);
 /* The reference's <prefix>_dos.csv, byte for byte. */
 wlg_status wlg_write_dos_csv(const char* path, double emin, double width, uint64_t bins, const double* log_g,
                              const uint64_t* histogram, const double* standard_error, const uint8_t* valid);

@@ -147,6 +147,8 @@ class Oracle(_Checker):
             "orc_walker_counters": (None, [_vp, P(_u64)]),
             "orc_walker_pilot": (None, [_vp, P(_dbl), P(_u64), P(_u64), P(_dbl), P(C.c_int8), P(C.c_uint8)]),
             "orc_run_rewl": (_vp, [_vp, P(_abi.wlg_run_config), _cp, _sz]),
+            "orc_run_rewl_warm": (_vp, [_vp, P(_abi.wlg_run_config), P(_dbl), _dbl, C.c_int, _cp, _sz]),
+            "orc_walker_warm_start": (None, [_vp, P(_dbl), _dbl, C.c_int]),
             "orc_result_destroy": (None, [_vp]),
             "orc_result_totals": (None, [_vp, P(_abi.wlg_run_totals)]),
             "orc_result_fragment": (C.c_int, [_vp, _u64, P(_dbl), P(_u64), P(_dbl), P(C.c_uint8)]),
@@ -236,12 +238,19 @@ class Oracle(_Checker):
                spins: Optional[np.ndarray] = None) -> "CheckerWalker":
         return CheckerWalker(self, system, walker_id, emin, emax, width, window, params, seed, spins)
 
-    def run_rewl(self, system: System, config: RunConfig) -> RewlResult:
+    def run_rewl(self, system: System, config: RunConfig, warm_start=None) -> RewlResult:
+        """run_rewl; warm_start = (log_g over the grid, factor, continue_schedule) applies the
+        engine's warm start to every walker after construction."""
         h = self._couplings(system)
         try:
             c, keep = config._struct(system.size())
             err = _err()
-            r = self.lib.orc_run_rewl(h, C.byref(c), err, len(err))
+            if warm_start is None:
+                r = self.lib.orc_run_rewl(h, C.byref(c), err, len(err))
+            else:
+                lg = np.ascontiguousarray(warm_start[0], dtype=np.float64)
+                r = self.lib.orc_run_rewl_warm(h, C.byref(c), _dptr(lg), float(warm_start[1]),
+                                               1 if warm_start[2] else 0, err, len(err))
             if not r:
                 raise CheckerError(6, err.value.decode())
             try:
@@ -495,6 +504,13 @@ class CheckerWalker:
         if self.p != "orc":
             raise CheckerError(1, "only the restatement has the FP32 update")
         self.L.orc_couplings_set_update_fp32(self._coup, 1 if on else 0)
+
+    def warm_start(self, log_g: np.ndarray, factor: float, continue_schedule: bool = False):
+        """The engine's warm start (restatement only; the reference has none)."""
+        if self.p != "orc":
+            raise CheckerError(7, "the reference has no warm start")
+        self._warm = np.ascontiguousarray(log_g, dtype=np.float64)
+        self.L.orc_walker_warm_start(self.h, _dptr(self._warm), float(factor), 1 if continue_schedule else 0)
 
     def run_attempts(self, count: int):
         err = _err()

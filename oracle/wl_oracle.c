@@ -345,6 +345,7 @@ struct orc_walker {
     uint64_t active_count, refine_count;
     double factor;
     uint64_t attempted, accepted, forced, last_acc;
+    uint64_t time_offset; /* 1/t: f = active / (attempted + time_offset); 0: the reference's rule */
     int stage;
     uint8_t rt_state;
     uint64_t round_trips;
@@ -355,6 +356,9 @@ struct orc_walker {
 
 static int64_t w_index(const orc_walker* w, double e) { return orc_grid_index(w->gmin, w->gmax, w->gw, e); }
 static int w_contains(const orc_walker* w, int64_t b) { return b >= 0 && (uint64_t)b >= w->wb && (uint64_t)b < w->we; }
+
+/* time_offset of a warm-started walker whose first covered check continues the schedule */
+#define ORC_CONTINUE_SCHEDULE (~(uint64_t)0)
 
 /* update_current_bin (wang_landau.cpp:290-303) */
 static int update_current_bin(orc_walker* w, char* err, size_t len) {
@@ -371,7 +375,7 @@ static int update_current_bin(orc_walker* w, char* err, size_t len) {
 static void update_inverse_time_factor(orc_walker* w) {
     if (w->stage != WLG_STAGE_INVERSE_TIME) return;
     const uint64_t count = w->active_count;
-    if (count != 0 && w->attempted != 0) w->factor = (double)count / (double)w->attempted;
+    if (count != 0 && w->attempted != 0) w->factor = (double)count / (double)(w->attempted + w->time_offset);
     if (w->factor <= w->p.final_factor) w->stage = WLG_STAGE_FROZEN;
 }
 
@@ -677,8 +681,18 @@ int orc_walker_begin_next_iteration(orc_walker* w, char* err, size_t len) {
         w->refine_count = 0;
     }
     if (w->p.inverse_time_enabled) {
-        const double inverse_time = w->attempted == 0 ? 1.0 : (double)w->active_count / (double)w->attempted;
-        if (w->factor <= inverse_time) { w->stage = WLG_STAGE_INVERSE_TIME; w->factor = inverse_time; }
+        if (w->time_offset == ORC_CONTINUE_SCHEDULE) {
+            /* warm start continuing the schedule: 1/t from the factor reached, as if
+             * round(active / factor) attempts had been made */
+            const double made = nearbyint((double)w->active_count / w->factor);
+            const double attempted = (double)w->attempted;
+            w->time_offset = made > attempted ? (uint64_t)(made - attempted) : 0;
+            w->stage = WLG_STAGE_INVERSE_TIME;
+        } else {
+            const double inverse_time =
+                w->attempted == 0 ? 1.0 : (double)w->active_count / (double)(w->attempted + w->time_offset);
+            if (w->factor <= inverse_time) { w->stage = WLG_STAGE_INVERSE_TIME; w->factor = inverse_time; }
+        }
     }
     if (w->factor <= w->p.final_factor) w->stage = WLG_STAGE_FROZEN;
     return 0;
@@ -1002,7 +1016,19 @@ static int check_precision(const wlg_run_config* cfg, char* err, size_t len) {
     return 0;
 }
 
+void orc_walker_warm_start(orc_walker* w, const double* log_g, double factor, int continue_schedule) {
+    for (uint64_t b = w->wb; b < w->we; ++b) w->log_g[b] = log_g[b];
+    w->factor = factor;
+    w->stage = factor <= w->p.final_factor ? WLG_STAGE_FROZEN : WLG_STAGE_WANG_LANDAU;
+    w->time_offset = continue_schedule ? ORC_CONTINUE_SCHEDULE : 0;
+}
+
 orc_result* orc_run_rewl(const orc_couplings* c, const wlg_run_config* cfg, char* err, size_t len) {
+    return orc_run_rewl_warm(c, cfg, NULL, 0.0, 0, err, len);
+}
+
+orc_result* orc_run_rewl_warm(const orc_couplings* c, const wlg_run_config* cfg, const double* warm_log_g,
+                              double warm_factor, int continue_schedule, char* err, size_t len) {
     if (validate_config(cfg, 0, err, len)) return NULL;
     if (check_precision(cfg, err, len)) return NULL;
     uint64_t bins = 0;
@@ -1033,6 +1059,8 @@ orc_result* orc_run_rewl(const orc_couplings* c, const wlg_run_config* cfg, char
                 return NULL;
             }
         }
+    if (warm_log_g)
+        for (uint64_t q = 0; q < total; ++q) orc_walker_warm_start(ws[q], warm_log_g, warm_factor, continue_schedule);
     /* FP32 couplings: the constructors above used FP64; the updates from here on use FP32 */
     const int saved_update_fp32 = c->update_fp32;
     if (cfg->coupling_precision == WLG_PRECISION_FP32) ((orc_couplings*)c)->update_fp32 = 1;

@@ -63,9 +63,21 @@ void orc_walker_pilot(const orc_walker* w, double* squared_displacement, uint64_
                       uint64_t* round_trips, double* representative_energies,
                       int8_t* representative_spins, uint8_t* representative_present);
 
+/* Not in the reference: the engine's warm start (wlg_engine_warm_start and
+ * wlg_engine_warm_start_continue).  Before the first attempt, the window slice of log g is
+ * set from log_g (whole grid), ln f to factor (frozen at once if <= final_factor).  With
+ * continue_schedule the first covered check (begin_next_iteration, src/wang_landau.cpp:
+ * 389-409) halves ln f and enters the 1/t stage at once, counting round(active / factor) -
+ * attempted attempts as already made: f = active / (attempted + offset) from then on
+ * (update_inverse_time_factor, src/wang_landau.cpp:309-315, with the offset added). */
+void orc_walker_warm_start(orc_walker* w, const double* log_g, double factor, int continue_schedule);
+
 /* run_rewl, serial path (src/parallel.cpp:276-747) */
 orc_result* orc_run_rewl(const orc_couplings* c, const wlg_run_config* config, char* err,
                          size_t errlen);
+/* run_rewl with every walker warm-started (orc_walker_warm_start) after construction. */
+orc_result* orc_run_rewl_warm(const orc_couplings* c, const wlg_run_config* config, const double* log_g,
+                              double factor, int continue_schedule, char* err, size_t errlen);
 void orc_result_destroy(orc_result* r);
 void orc_result_totals(const orc_result* r, wlg_run_totals* out);
 int orc_result_fragment(const orc_result* r, uint64_t w, double* log_g, uint64_t* histogram,

@@ -290,6 +290,7 @@ SIGNATURES = {
     "wlg_engine_warm_start_continue": (_i32, [_vp, P(_dbl), _dbl]),
     "wlg_stitch_dos": (_i32, [_dbl, _dbl, _dbl, P(wlg_fragment_view), _u64, _i32, _u64, P(_dbl), P(_u64), P(_dbl),
                                P(C.c_uint8), P(wlg_join_quality), P(_i32)]),
+    "wlg_engine_stitch": (_i32, [_vp, _i32, P(_dbl), P(_u64), P(_dbl), P(C.c_uint8), P(wlg_join_quality), P(_i32)]),
     "wlg_write_dos_csv": (_i32, [C.c_char_p, _dbl, _dbl, _u64, P(_dbl), P(_u64), P(_dbl), P(C.c_uint8)]),
     "wlg_write_fragment_csv": (_i32, [C.c_char_p, _dbl, _dbl, _u64, _u64, _u64, P(_dbl), P(_u64), P(_dbl),
                                       P(C.c_uint8)]),

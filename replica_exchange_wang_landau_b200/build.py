@@ -20,7 +20,7 @@ PACKAGE = Path(__file__).resolve().parent
 CSRC = PACKAGE / "csrc"
 BUILD = PACKAGE / "_build"
 LIBRARY = PACKAGE / "libwlg.so"
-SOURCES = ["physics.cu", "walker.cu", "sweep.cu", "sweep_csr.cu", "sweep_window.cu", "rewl.cu", "precision.cu", "mlp.cu", "noalloc.cu", "engine.cpp", "host.cpp", "stitch.cpp", "adaptive.cpp", "api.cpp"]
+SOURCES = ["physics.cu", "walker.cu", "sweep.cu", "sweep_csr.cu", "sweep_window.cu", "rewl.cu", "stitch.cu", "precision.cu", "mlp.cu", "noalloc.cu", "engine.cpp", "host.cpp", "stitch.cpp", "adaptive.cpp", "api.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -325,6 +325,17 @@ void wlg_engine_destroy(wlg_engine* engine) {
     if (cudaSetDevice((engine)->impl->device) != cudaSuccess)                                    \
         return fail(WLG_ERR_DEVICE, "cannot select the engine's CUDA device");
 
+wlg_status wlg_engine_stitch(wlg_engine* engine, int32_t complete_range, double* log_g, uint64_t* histogram,
+                             double* standard_error, uint8_t* valid, wlg_join_quality* joins,
+                             int32_t* fully_normalized) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] {
+        if (!log_g || !histogram || !standard_error || !valid)
+            throw wlg::WlgError(WLG_ERR_INVALID_ARGUMENT, "null output array");
+        engine->impl->stitch(complete_range, log_g, histogram, standard_error, valid, joins, fully_normalized);
+    });
+}
+
 wlg_status wlg_engine_inject_wait_timeout(wlg_engine* engine) {
     WLG_ENGINE_GUARD(engine)
     return guarded([&] { engine->impl->inject_wait_timeout(); });

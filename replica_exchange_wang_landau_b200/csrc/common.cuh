@@ -240,10 +240,13 @@ struct alignas(16) WalkerState {
     int32_t rt_state;      // round-trip state machine
     int32_t rep_pending;   // representatives must be refreshed before the next batch
     // 1/t stage: attempts counted as made before this run, f = active / (attempted +
-    // time_offset).  0 is the reference's rule; a warm start that continues the schedule
-    // (wlg_engine_warm_start_continue) sets window bins / ln f of the start.
+    // time_offset).  0 is the reference's rule.  A warm start that continues the schedule
+    // (wlg_engine_warm_start_continue) sets kContinueSchedule; the first covered check then
+    // enters the 1/t stage at the factor reached and sets the offset that makes the 1/t
+    // factor start there.
     uint64_t time_offset;
 };
+constexpr uint64_t kContinueSchedule = ~0ULL;
 
 // Run-wide control block written by the kernels and read by the host.
 struct alignas(16) Control {

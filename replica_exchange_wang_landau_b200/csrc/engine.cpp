@@ -975,6 +975,70 @@ void Engine::fragments(int allow_empty, double* log_g, uint64_t* hist, double* s
         if (st) throw WlgError(WLG_ERR_RUNTIME, "Walkers in an energy window have no common active bin");
 }
 
+void Engine::stitch(int complete_range, double* log_g, uint64_t* hist, double* sem, uint8_t* valid,
+                    wlg_join_quality* joins, int32_t* fully_normalized) {
+    const size_t WB = windows_ * bins_, B = bins_;
+    const size_t status_at = ((25 * WB + 15) / 16) * 16;
+    if (!d_frag_.ptr) d_frag_.allocate(status_at + 4 * windows_);
+    char* base = d_frag_.get<char>();
+    double* d_lg = reinterpret_cast<double*>(base);
+    uint64_t* d_h = reinterpret_cast<uint64_t*>(base + 8 * WB);
+    double* d_se = reinterpret_cast<double*>(base + 16 * WB);
+    uint8_t* d_v = reinterpret_cast<uint8_t*>(base + 24 * WB);
+    int* d_status = reinterpret_cast<int*>(base + status_at);
+    // the stitched arrays, the joins and the status word
+    const size_t joins_at = ((25 * B + 15) / 16) * 16;
+    const size_t stitch_status_at = joins_at + sizeof(wlg_join_quality) * windows_;
+    if (!d_stitch_.ptr) d_stitch_.allocate(stitch_status_at + 16);
+    char* out = d_stitch_.get<char>();
+    double* o_lg = reinterpret_cast<double*>(out);
+    uint64_t* o_h = reinterpret_cast<uint64_t*>(out + 8 * B);
+    double* o_se = reinterpret_cast<double*>(out + 16 * B);
+    uint8_t* o_v = reinterpret_cast<uint8_t*>(out + 24 * B);
+    wlg_join_quality* o_j = reinterpret_cast<wlg_join_quality*>(out + joins_at);
+    int* o_status = reinterpret_cast<int*>(out + stitch_status_at);
+    launch_summarize(view_, 0, static_cast<int>(windows_), 0, d_lg, d_h, d_se, d_v, d_status, stream_);
+    launch_stitch(static_cast<int>(windows_), static_cast<int>(B), view_.win_begin, view_.win_end, d_lg, d_h, d_se, d_v,
+                  d_status, cfg_.bin_width, complete_range, o_lg, o_h, o_se, o_v, o_j, o_status, stream_);
+    int status = 0;
+    std::vector<wlg_join_quality> q(windows_ > 1 ? windows_ - 1 : 0);
+    check_cuda(cudaMemcpyAsync(log_g, o_lg, B * 8, cudaMemcpyDeviceToHost, stream_), "copy");
+    check_cuda(cudaMemcpyAsync(hist, o_h, B * 8, cudaMemcpyDeviceToHost, stream_), "copy");
+    check_cuda(cudaMemcpyAsync(sem, o_se, B * 8, cudaMemcpyDeviceToHost, stream_), "copy");
+    check_cuda(cudaMemcpyAsync(valid, o_v, B, cudaMemcpyDeviceToHost, stream_), "copy");
+    if (!q.empty())
+        check_cuda(cudaMemcpyAsync(q.data(), o_j, q.size() * sizeof(wlg_join_quality), cudaMemcpyDeviceToHost, stream_),
+                   "copy");
+    check_cuda(cudaMemcpyAsync(&status, o_status, sizeof status, cudaMemcpyDeviceToHost, stream_), "copy");
+    check_cuda(cudaStreamSynchronize(stream_), "stitch");
+    switch (status) {
+        case 0: break;
+        case kStitchNoCommonBin: throw WlgError(WLG_ERR_RUNTIME, "Walkers in an energy window have no common active bin");
+        case kStitchNoOverlap:
+            throw WlgError(WLG_ERR_INVALID_ARGUMENT, "DOS fragments must overlap and match the global grid");
+        case kStitchNoCommonOverlapBin:
+            throw WlgError(WLG_ERR_RUNTIME, "Adjacent DOS fragments have no common valid overlap bin");
+        case kStitchIncomplete:
+            throw WlgError(WLG_ERR_RUNTIME, "Complete-range normalization requires every DOS bin to be valid");
+        case kStitchNoValidBins: throw WlgError(WLG_ERR_RUNTIME, "Stitched DOS has no valid bins");
+        default: throw WlgError(WLG_ERR_DEVICE, "stitch_kernel failed");
+    }
+    if (complete_range) {
+        // N ln 2 - log sum exp, with the C library's exp and log (as the reference computes it)
+        double top = -std::numeric_limits<double>::infinity();
+        for (size_t i = 0; i < B; ++i)
+            if (std::isfinite(log_g[i])) top = std::max(top, log_g[i]);
+        double sum = 0.0;
+        for (size_t i = 0; i < B; ++i)
+            if (std::isfinite(log_g[i])) sum += std::exp(log_g[i] - top);
+        const double shift = static_cast<double>(sys_.n) * std::log(2.0) - (top + std::log(sum));
+        for (size_t i = 0; i < B; ++i)
+            if (valid[i] != 0) log_g[i] += shift;
+    }
+    if (joins) std::copy(q.begin(), q.end(), joins);
+    if (fully_normalized) *fully_normalized = complete_range ? 1 : 0;
+}
+
 void Engine::sampling(uint64_t w, double* sq, uint64_t* samples, uint64_t* round_trips, uint64_t* walkers) {
     if (w >= windows_) throw WlgError(WLG_ERR_OUT_OF_RANGE, "window index out of range");
     if (!p_.collect) throw WlgError(WLG_ERR_LOGIC, "window statistics were not collected");
@@ -1266,14 +1330,8 @@ void Engine::warm_start(const double* log_g, double factor, bool continue_schedu
         for (uint64_t b = win_[2 * st.window]; b < win_[2 * st.window + 1]; ++b) grid[k * bins_ + b] = log_g[b];
         states[k].factor = factor;
         states[k].stage = factor <= p_.final_factor ? kFrozen : kWangLandau;
-        // continuing the 1/t schedule: the attempts a 1/t run over the window's bins would
-        // have made to reach ln f = factor count as made before the run
-        const double offset = continue_schedule
-                                  ? std::nearbyint(static_cast<double>(win_[2 * st.window + 1] - win_[2 * st.window]) / factor)
-                                  : 0.0;
-        if (!(offset < 0x1.0p62))
-            throw WlgError(WLG_ERR_INVALID_ARGUMENT, "The warm-start factor is too small to continue the 1/t schedule");
-        states[k].time_offset = static_cast<uint64_t>(offset);
+        // continuing the 1/t schedule: the offset is set at the first covered check
+        states[k].time_offset = continue_schedule ? kContinueSchedule : 0;
     }
     check_cuda(cudaMemcpyAsync(d_log_g_.ptr, grid.data(), grid.size() * sizeof(double), cudaMemcpyHostToDevice,
                                stream_),

@@ -201,6 +201,16 @@ void launch_flush_pending(const EngineView& v, cudaStream_t stream);
 // summarize_impl for windows [window, window + windows): outputs window-major, bins each
 void launch_summarize(const EngineView& v, int window, int windows, int allow_empty, double* log_g, uint64_t* hist,
                       double* sem, uint8_t* valid, int* status, cudaStream_t stream);
+// stitch.cu: stitch_dos on the fragments summarize_kernel left on the device.  Status codes:
+constexpr int kStitchNoCommonBin = 1;          // "Walkers in an energy window have no common active bin"
+constexpr int kStitchNoOverlap = 2;            // "DOS fragments must overlap and match the global grid"
+constexpr int kStitchNoCommonOverlapBin = 3;   // "Adjacent DOS fragments have no common valid overlap bin"
+constexpr int kStitchIncomplete = 4;           // "Complete-range normalization requires every DOS bin to be valid"
+constexpr int kStitchNoValidBins = 5;          // "Stitched DOS has no valid bins"
+void launch_stitch(int windows, int bins, const int32_t* wbeg, const int32_t* wend, const double* flg,
+                   const uint64_t* fh, const double* fse, const uint8_t* fv, const int* summarize_status,
+                   double width, int complete_range, double* lg, uint64_t* h, double* se, uint8_t* ok,
+                   wlg_join_quality* joins, int* status, cudaStream_t stream);
 void launch_sampling(const EngineView& v, int window, double* sq, uint64_t* samples, uint64_t* trips,
                      cudaStream_t stream);
 void launch_walker_statistics(const EngineView& v, wlg_walker_statistics* out, cudaStream_t stream);
@@ -268,6 +278,10 @@ class Engine {
     void fragment(uint64_t w, int allow_empty, double* log_g, uint64_t* hist, double* sem, uint8_t* valid);
     // every window's fragment in one launch and one copy (arrays windows x bins, window-major)
     void fragments(int allow_empty, double* log_g, uint64_t* hist, double* sem, uint8_t* valid);
+    // stitch_dos of every window's fragment on the device (whole-grid outputs, bins entries;
+    // joins: windows - 1 entries or NULL)
+    void stitch(int complete_range, double* log_g, uint64_t* hist, double* sem, uint8_t* valid,
+                wlg_join_quality* joins, int32_t* fully_normalized);
     void sampling(uint64_t w, double* sq, uint64_t* samples, uint64_t* round_trips, uint64_t* walkers);
     void walker_statistics(wlg_walker_statistics* out, uint64_t capacity);
     void representatives(double* energies, int8_t* spins, uint64_t capacity, uint64_t* count);
@@ -280,9 +294,9 @@ class Engine {
     double exchange_log_probability(uint64_t left, uint64_t right);
     void swap(uint64_t left, uint64_t right);
     void precision_report(wlg_precision_report* out);
-    // continue_schedule: each walker's 1/t stage counts window bins / factor attempts as made
-    // before the run (f = active / (attempted + offset)), so the factor never rises above the
-    // warm start's; false keeps the reference's rule (f = active / attempted).
+    // continue_schedule: the first covered check enters the 1/t stage at the factor reached and
+    // counts round(active / factor) attempts as made (f = active / (attempted + offset)), so
+    // the factor never rises above the warm start's; false keeps the reference's rule.
     void warm_start(const double* log_g, double factor, bool continue_schedule = false);
     // every walker's state, the control block and the recompute schedule (multi-walker
     // checkpoint; the reference checkpoints single-walker runs only)
@@ -339,7 +353,7 @@ class Engine {
 
     DeviceBuffer d_win_begin_, d_win_end_, d_ws_, d_log_g_, d_hist_, d_active_, d_refine_, d_sqdisp_,
         d_dsamples_, d_spins_, d_fields_, d_rep_energy_, d_rep_dist_, d_rep_target_, d_rep_present_,
-        d_rep_spins_, d_ctl_, d_scratch_, d_frag_;
+        d_rep_spins_, d_ctl_, d_scratch_, d_frag_, d_stitch_;
     // mixed precision: FP64 recompute every recompute_epochs_ epochs (0 = never)
     DeviceBuffer d_rfields_, d_renergy_, d_prec_;
     uint64_t recompute_epochs_ = 0, next_recompute_ = 0;

@@ -107,12 +107,21 @@ __device__ __forceinline__ void warp_begin_next_iteration(WalkerState& st, uint6
         st.refine_count = 0;
     }
     if (p.inverse_time) {
-        const double inverse_time =
-            st.attempted == 0 ? 1.0
-                              : static_cast<double>(st.active_count) / static_cast<double>(st.attempted + st.time_offset);
-        if (st.factor <= inverse_time) {
+        if (st.time_offset == kContinueSchedule) {
+            // a warm start continuing the schedule: the 1/t stage starts at this check from the
+            // factor reached, as if round(active / factor) attempts had been made
+            const double made = nearbyint(static_cast<double>(st.active_count) / st.factor);
+            const double attempted = static_cast<double>(st.attempted);
+            st.time_offset = made > attempted ? static_cast<uint64_t>(made - attempted) : 0;
             st.stage = kInverseTime;
-            st.factor = inverse_time;
+        } else {
+            const double inverse_time = st.attempted == 0 ? 1.0
+                                                          : static_cast<double>(st.active_count) /
+                                                                static_cast<double>(st.attempted + st.time_offset);
+            if (st.factor <= inverse_time) {
+                st.stage = kInverseTime;
+                st.factor = inverse_time;
+            }
         }
     }
     if (st.factor <= p.final_factor) st.stage = kFrozen;

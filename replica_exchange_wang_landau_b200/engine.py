@@ -681,6 +681,20 @@ class Engine:
         return [DosFragment(self.window(w), lg[w * B:(w + 1) * B].copy(), h[w * B:(w + 1) * B].copy(),
                             se[w * B:(w + 1) * B].copy(), v[w * B:(w + 1) * B].copy()) for w in range(W)]
 
+    def stitch(self, complete_range: bool = False) -> "DensityOfStates":
+        """stitch_dos (src/analysis.cpp:45-130) of every window's fragment, on the device."""
+        c = self.config
+        lg, se = np.empty(self.bins), np.empty(self.bins)
+        h, ok = np.empty(self.bins, np.uint64), np.empty(self.bins, np.uint8)
+        count = int(c.windows)
+        joins = (_abi.wlg_join_quality * max(1, count - 1))()
+        full = C.c_int32(0)
+        _check(self._lib.wlg_engine_stitch(self._h, int(complete_range), _dptr(lg), _u64ptr(h), _dptr(se), _u8ptr(ok),
+                                           joins, C.byref(full)))
+        q = [{name: getattr(joins[k], name) for name, _ in _abi.wlg_join_quality._fields_} for k in range(count - 1)]
+        return DensityOfStates(c.emin, c.emax, c.bin_width, lg, h, se, ok, [j["join_bin"] for j in q], q,
+                               bool(full.value))
+
     def sampling_statistics(self, w: int) -> WindowSamplingStatistics:
         B = self.bins
         sq, ds = np.zeros(B), np.zeros(B, np.uint64)

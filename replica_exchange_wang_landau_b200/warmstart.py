@@ -305,3 +305,100 @@ def run_to_accuracy(system: System, emin: float, emax: float, width: float, refe
             if t["converged"] or per_walker >= max_attempts:
                 break
     return {"warm": warm, "attempts": hit_attempts, "seconds": hit_seconds, "final_error": err}
+
+
+# ---- the learned configuration: generated dilute systems and time to accuracy -----------
+
+
+def dilute_instance(k: int, seed0: int = 50_000):
+    """The k-th generated system of the learned configuration: N uniform in 64..1024, random
+    sequential addition in a periodic cube at density 0.3-0.8 (minimum separation 0.8),
+    random-sphere axes; one grid over about +-4 sigma of the random-configuration energy
+    distribution (sigma^2 = sum_{i<j} J_ij^2) in 200 power-of-two bins.
+    Returns (system, emin, emax, width)."""
+    from .geometry import random_sequential
+    rng = np.random.default_rng(seed0 + k)
+    n = int(rng.integers(64, 1025))
+    s = System(random_sequential(n, float(rng.uniform(0.3, 0.8)), 0.8, seed=seed0 + k), 1.0, 0.0)
+    sigma = math.sqrt(0.5 * float(np.sum(s.couplings("fp64") ** 2)))
+    w = 2.0 ** round(math.log2(8.0 * sigma / 200.0))
+    return s, -100.0 * w, 100.0 * w, w
+
+
+def accuracy_error(log_g: np.ndarray, valid: np.ndarray, judge_log_g: np.ndarray) -> float:
+    """max |d - mean(d)| with d = log g - judge over the bins the judge found (inf until all of
+    them are valid in the run)."""
+    ref = np.asarray(judge_log_g, dtype=np.float64)
+    occ = np.isfinite(ref)
+    if not np.all(np.asarray(valid)[occ] == 1):
+        return math.inf
+    d = np.asarray(log_g, dtype=np.float64)[occ] - ref[occ]
+    return float(np.max(np.abs(d - d.mean())))
+
+
+def single_window_config(emin: float, emax: float, width: float, n: int, seed: int, final_factor: float,
+                         walkers: int = 2, precision: str = "fp64") -> RunConfig:
+    """One window of `walkers` walkers, 1/t Wang-Landau to final_factor, exchange interval 10 MCS
+    (the epoch), FP64 recompute once per epoch for FP32 / BF16 couplings."""
+    c = RunConfig(emin=emin, emax=emax, bin_width=width, windows=1, walkers=walkers, seed=seed)
+    c.wl = WlParameters(0.8, 100, final_factor, 1000, 0, True)
+    c.exchange_interval_mcs = 10.0
+    c.max_mcs = 0.0
+    c.coupling_precision = precision
+    c.recompute_interval_mcs = 10.0
+    c.resolve_mcs(n)
+    return c
+
+
+def batch_to_accuracy(engines: Sequence[Engine], judges: Sequence[np.ndarray], tolerance: float,
+                      chunk_epochs: int = 8, max_seconds: float = 600.0) -> dict:
+    """Advances the engines together (one Batch: one CUDA-graph launch per step for all of them)
+    and, every chunk_epochs epochs, measures each engine's error against its judge.  Returns the
+    wall seconds and attempts per walker at which each engine first met the tolerance (None if
+    not within max_seconds), the seconds until all had, and each engine's attempts per second
+    over the run."""
+    import time
+
+    from .engine import Batch
+    hit_s = [None] * len(engines)
+    hit_att = [None] * len(engines)
+    errors = [math.inf] * len(engines)
+    with Batch(engines) as batch:
+        t0 = time.perf_counter()
+        while True:
+            batch.run_epochs(chunk_epochs)
+            now = time.perf_counter() - t0
+            for k, (e, judge) in enumerate(zip(engines, judges)):
+                if hit_s[k] is not None:
+                    continue
+                frag = e.fragment(0, allow_empty=True)
+                errors[k] = accuracy_error(frag.log_g, frag.valid, judge)
+                if errors[k] <= tolerance:
+                    hit_s[k] = now
+                    hit_att[k] = e.totals()["attempted"] // e.walkers
+            if all(h is not None for h in hit_s) or now > max_seconds:
+                break
+        elapsed = time.perf_counter() - t0
+    rates = [e.totals()["attempted"] / e.walkers / elapsed for e in engines]
+    done = [h for h in hit_s if h is not None]
+    return {"hit_seconds": hit_s, "hit_attempts_per_walker": hit_att, "final_errors": errors,
+            "all_seconds": max(done) if len(done) == len(engines) else None, "reached": len(done),
+            "attempts_per_walker_per_s": rates, "elapsed_s": elapsed}
+
+
+def engine_to_accuracy(engine: Engine, judge: np.ndarray, tolerance: float, chunk_epochs: int = 8,
+                       max_seconds: float = 120.0) -> dict:
+    """One engine alone, chunk_epochs epochs at a time, until its error meets the tolerance."""
+    import time
+    t0 = time.perf_counter()
+    err = math.inf
+    while True:
+        engine.run_epochs(chunk_epochs)
+        frag = engine.fragment(0, allow_empty=True)
+        err = accuracy_error(frag.log_g, frag.valid, judge)
+        now = time.perf_counter() - t0
+        if err <= tolerance or now > max_seconds:
+            break
+    att = engine.totals()["attempted"] // engine.walkers
+    return {"seconds": now if err <= tolerance else None, "attempts_per_walker": att if err <= tolerance else None,
+            "attempts_per_walker_per_s": att / now, "final_error": err}

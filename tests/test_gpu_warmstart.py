@@ -8,6 +8,7 @@ import math
 import numpy as np
 import pytest
 
+from helpers import results_equal
 from oracle import mlp_oracle
 from replica_exchange_wang_landau_b200.engine import Engine, Geometry, InvalidArgument, LogicError, RunConfig, System
 from replica_exchange_wang_landau_b200.geometry import random_sequential
@@ -104,3 +105,51 @@ def test_learned_warm_start_ablation(oracle):
         flat += a["attempts"]
         learned += b["attempts"]
     assert 0.5 * flat <= learned <= 1.5 * flat, (learned, flat)
+
+
+def _warm_grid(c: RunConfig, scale: float) -> np.ndarray:
+    """A smooth, finite warm-start estimate over the whole grid."""
+    bins = c.bins()
+    x = np.linspace(-1.0, 1.0, bins)
+    return -scale * x * x
+
+
+WARM_RUNS = {
+    # dense split sweep with exchanges, three windows of two walkers
+    "dense27": (lambda: System(Geometry.simple_cubic(3, 3, 3, periodic=True)),
+                dict(emin=-60, emax=60, bin_width=0.5, windows=3, walkers=2, seed=21, max_mcs=600,
+                     exchange_interval_mcs=1, check_interval_mcs=10)),
+    # the single-window kernel (8 sites, one window of two walkers)
+    "window8": (lambda: System(Geometry.simple_cubic(2, 2, 2, periodic=False)),
+                dict(emin=-20, emax=20, bin_width=0.25, windows=1, walkers=2, seed=1234, max_mcs=20000,
+                     check_interval_mcs=50)),
+    # the CSR sweep
+    "csr64": (lambda: System(Geometry.simple_cubic(4, 4, 4, periodic=True), 1.0, 1.8),
+              dict(emin=-150, emax=150, bin_width=0.5, windows=2, walkers=3, seed=9, max_mcs=300,
+                   exchange_interval_mcs=1, check_interval_mcs=5)),
+}
+
+
+@pytest.mark.parametrize("continue_schedule", [False, True])
+@pytest.mark.parametrize("name", list(WARM_RUNS))
+def test_warm_started_run_bitwise(oracle, name, continue_schedule):
+    """run_rewl after a warm start at ln f = 1e-3, with the reference's 1/t rule and with the
+    schedule continued (f = active / (attempted + window bins / 1e-3)), bit for bit against the
+    oracle's restatement; the continued schedule's factor never exceeds the start's."""
+    make_system, kw = WARM_RUNS[name]
+    s = make_system()
+    c = RunConfig(**kw)
+    c.wl.final_factor = 1e-6
+    c.resolve_mcs(s.size())
+    lg = _warm_grid(c, 3.0)
+    with Engine(s, c) as e:
+        e.warm_start(lg, 1e-3, continue_schedule=continue_schedule)
+        e.run()
+        got = e.result()
+        stages = [e.snapshot(w).stage for w in range(e.walkers)]
+    want = oracle.run_rewl(s, c, warm_start=(lg, 1e-3, continue_schedule))
+    assert results_equal(got, want) == []
+    assert stages.count(1) + stages.count(2) > 0  # the 1/t stage was reached
+    factors = [st["factor"] for st in got.walker_statistics]
+    if continue_schedule:
+        assert max(factors) <= 1e-3
