@@ -609,7 +609,7 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
                                      ("combined", "fp32", True)):
         engs = engines(precision, learned)
         try:
-            r = batch_to_accuracy(engs, judges, tolerance)
+            r = batch_to_accuracy(engs, judges, tolerance, max_seconds=150.0)
             r["ln_f_1e-8_s_extrapolated"] = to_ln_f_1e8(engs, r["attempts_per_walker_per_s"])
             if precision != "fp64":
                 reps = [e.precision_report() for e in engs]
@@ -630,7 +630,7 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
     for k in range(sequential_sample):
         s, lo, hi, w = held[k]
         with Engine(s, single_window_config(lo, hi, w, s.size(), 20_000 + k, 1e-8)) as e:
-            r = engine_to_accuracy(e, judges[k], tolerance)
+            r = engine_to_accuracy(e, judges[k], tolerance, max_seconds=40.0)
             active = float(np.mean([x["active_bins"] for x in e.walker_statistics()]))
         r["ln_f_1e-8_s"] = active / 1e-8 / r["attempts_per_walker_per_s"]
         r["active_bins"] = active
@@ -695,6 +695,60 @@ def c1_config():
     c.wl.final_factor = 1e-8
     c.resolve_mcs(g.size())
     return System(g, 1.0, 0.0), c
+
+
+def c1_converged_line() -> dict:
+    """The plain configuration run to ln f <= 1e-8 and timed, not extrapolated: the engine on the
+    GPU (the single-window kernel) and, started at the same moment, the reference's own wl_run
+    on two host threads (one per walker) with the same command-line configuration.  Each run's
+    merged log g is compared with the exact density of states (enumeration of the 256
+    configurations) as max |d - mean(d)| over the exactly occupied bins."""
+    from oracle.oracle import Oracle
+    from replica_exchange_wang_landau_b200.engine import Engine
+    system, config = c1_config()
+    config.max_mcs = 0.0
+    config.resolved_spin_count = 0
+    config.resolve_mcs(system.size())
+    counts = Oracle().exact_counts(system, config.emin, config.emax, config.bin_width)
+    occ = counts > 0
+    exact = np.log(counts[occ].astype(float))
+
+    def error(log_g) -> float:
+        d = np.asarray(log_g, dtype=np.float64)[occ] - exact
+        return float(np.max(np.abs(d - d.mean())))
+
+    tmp = tempfile.TemporaryDirectory()
+    ref = None
+    if REFERENCE_WL_RUN.exists():
+        cmd = [str(REFERENCE_WL_RUN), "--nx", "2", "--ny", "2", "--nz", "2", "--periodic", "false", "--emin", "-20",
+               "--emax", "20", "--bin-width", "0.25", "--windows", "1", "--walkers", "2", "--final-factor", "1e-8",
+               "--seed", "1234", "--max-mcs", "0", "--output", str(Path(tmp.name) / "c1")]
+        ref = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                               env=dict(os.environ, OMP_NUM_THREADS="2"))
+    t0 = time.perf_counter()
+    with Engine(system, config) as e:
+        timing = e.time_run(1 << 40)
+        gpu_wall = time.perf_counter() - t0
+        totals = e.totals()
+        frag = e.fragments()[0]
+    out = {"workload": "2x2x2 open simple cubic, +z axes, dense FP64 J, [-20, 20] in bins of 0.25, 1 window x 2 "
+                       "walkers, 1/t to ln f = 1e-8, seed 1234",
+           "gpu": {"wall_s": gpu_wall, "device_s": timing["total_ms"] / 1e3, "converged": bool(totals["converged"]),
+                   "attempts_per_walker": totals["attempted"] // 2,
+                   "max_abs_dlog_g_vs_exact": error(frag.log_g)}}
+    if ref is not None:
+        stdout, _ = ref.communicate(timeout=7200)
+        summary = parse_wl_run_summary(stdout)
+        dos = np.genfromtxt(Path(tmp.name) / "c1_window_0.csv", delimiter=",", names=True)
+        lg = np.full(config.bins(), np.nan)
+        lg[dos["bin"].astype(int)] = dos["log_g"]
+        out["reference_cpu"] = {"elapsed_s": float(summary["elapsed_seconds"]), "threads": 2,
+                                "converged": summary["converged"] == "yes",
+                                "attempts_per_walker": int(summary["attempted_flips"]) // 2,
+                                "max_abs_dlog_g_vs_exact": error(lg),
+                                "program": "the reference's wl_run (oracle/_ref), OpenMP over the two walkers"}
+    tmp.cleanup()
+    return out
 
 
 def time_to_converge(value: float, cpu_value: float, active_bins: float, window_bins: float) -> dict:
@@ -831,11 +885,17 @@ def main() -> None:
                     help="print only the mixed-precision configuration's lines (N = 2458, FP64 / FP32 / BF16)")
     ap.add_argument("--csr-only", action="store_true",
                     help="print only the CSR configuration's line (the 32^3 lattice, 1024 walkers)")
+    ap.add_argument("--c1-converge", action="store_true",
+                    help="run the plain 8-spin configuration to ln f <= 1e-8 on the GPU and the reference's wl_run "
+                         "on the host at the same time, and print both (takes minutes)")
     ap.add_argument("--learned-only", action="store_true",
                     help="print only the learned configuration's time to accuracy (256 dilute systems)")
     args = ap.parse_args()
     if args.csr_only:
         print(json.dumps({"csr_batched": csr_batched_line()}))
+        return
+    if args.c1_converge:
+        print(json.dumps({"c1_converged": c1_converged_line()}))
         return
     if args.learned_only:
         print(json.dumps({"time_to_accuracy": learned_configuration_line()}))

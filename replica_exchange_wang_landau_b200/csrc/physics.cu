@@ -296,38 +296,39 @@ __global__ void fields_kernel(EngineView v, const int8_t* __restrict__ spins, in
     fields[k * field_stride + i] = sum;
 }
 
-// local_fields of dense couplings for kFieldGroup configurations per block.  Each thread owns
-// one site i and keeps kFieldGroup sums; the J column entries J[j][i] are read kFieldPrefetch
-// rows ahead into registers, and the configurations' spins are staged as doubles (+-1.0) in
-// shared memory, kFieldTile rows at a time, so that a term is one multiply and one add, with one
-// shared-memory broadcast (a double2) per two terms.  Every field is still summed sequentially over j with the reference's
-// operations (sum += J(i, j) * s_j, no contraction), so the result is the one of fields_kernel.
-constexpr int kFieldGroup = 8;      // configurations per block (16 measured slightly slower: fewer blocks)
-constexpr int kFieldTile = 256;     // rows j staged per pass (kFieldGroup x kFieldTile doubles = 16 KB)
+// local_fields of dense couplings for G configurations per block.  Each thread owns one site i
+// and keeps G sums; the J column entries J[j][i] are read kFieldPrefetch rows ahead into
+// registers, and the configurations' spins are staged as doubles (+-1.0) in shared memory,
+// TILE rows at a time, so that a term is one multiply and one add, with one shared-memory
+// broadcast (a double2) per two terms.  Every field is still summed sequentially over j with
+// the reference's operations (sum += J(i, j) * s_j, no contraction), so the result is the one
+// of fields_kernel whatever G is.  A block reads its sites' columns of J once for G
+// configurations: G = 8 keeps many blocks in flight for small counts; G = 32 reads J four times
+// less (the FP64 recompute of 256 walkers at N = 2458 read the 48 MB J 32 times with G = 8).
 constexpr int kFieldPrefetch = 8;   // rows of J in flight per thread
-constexpr int kFieldThreads = 128;
-__global__ void __launch_bounds__(kFieldThreads) fields_group_kernel(EngineView v, const int8_t* __restrict__ spins,
-                                                                      int64_t spin_stride, double* __restrict__ fields,
-                                                                      int64_t field_stride, int count) {
-    __shared__ __align__(16) double sigma[kFieldTile][kFieldGroup];  // row j: the group's spins, contiguous
+template <int G, int TILE, int THREADS>
+__global__ void __launch_bounds__(THREADS) fields_group_kernel(EngineView v, const int8_t* __restrict__ spins,
+                                                                int64_t spin_stride, double* __restrict__ fields,
+                                                                int64_t field_stride, int count) {
+    __shared__ __align__(16) double sigma[TILE][G];  // row j: the group's spins, contiguous
     const int n = v.n;
-    const int k0 = static_cast<int>(blockIdx.y) * kFieldGroup;
-    const int group = min(kFieldGroup, count - k0);
-    const int i = static_cast<int>(blockIdx.x) * kFieldThreads + static_cast<int>(threadIdx.x);
+    const int k0 = static_cast<int>(blockIdx.y) * G;
+    const int group = min(G, count - k0);
+    const int i = static_cast<int>(blockIdx.x) * THREADS + static_cast<int>(threadIdx.x);
     const bool site = i < n;
     const double* __restrict__ col = v.J64 + (site ? i : 0);  // J[j][i] at col[j * ld]
     const size_t ld = static_cast<size_t>(v.ld);
-    double sum[kFieldGroup];
+    double sum[G];
 #pragma unroll
-    for (int g = 0; g < kFieldGroup; ++g) sum[g] = 0.0;
+    for (int g = 0; g < G; ++g) sum[g] = 0.0;
     double jv[kFieldPrefetch];
 #pragma unroll
     for (int u = 0; u < kFieldPrefetch; ++u) jv[u] = u < n ? col[static_cast<size_t>(u) * ld] : 0.0;
-    for (int t0 = 0; t0 < n; t0 += kFieldTile) {
-        const int tile = min(kFieldTile, n - t0);
+    for (int t0 = 0; t0 < n; t0 += TILE) {
+        const int tile = min(TILE, n - t0);
         __syncthreads();  // the previous tile is no longer read
-        for (int q = static_cast<int>(threadIdx.x); q < kFieldGroup * kFieldTile; q += kFieldThreads) {
-            const int j = q / kFieldGroup, g = q % kFieldGroup;  // consecutive threads: one row, conflict-free stores
+        for (int q = static_cast<int>(threadIdx.x); q < G * TILE; q += THREADS) {
+            const int j = q / G, g = q % G;  // consecutive threads: one row, conflict-free stores
             sigma[j][g] = (g < group && j < tile)
                               ? static_cast<double>(spins[static_cast<size_t>(k0 + g) * spin_stride + t0 + j])
                               : 0.0;
@@ -346,7 +347,7 @@ __global__ void __launch_bounds__(kFieldThreads) fields_group_kernel(EngineView 
                 if (j0 + u < tile) {
                     const double2* row = reinterpret_cast<const double2*>(&sigma[j0 + u][0]);
 #pragma unroll
-                    for (int g2 = 0; g2 < kFieldGroup / 2; ++g2) {
+                    for (int g2 = 0; g2 < G / 2; ++g2) {
                         const double2 sg = row[g2];
                         sum[2 * g2] += jv[u] * sg.x;
                         sum[2 * g2 + 1] += jv[u] * sg.y;
@@ -359,7 +360,7 @@ __global__ void __launch_bounds__(kFieldThreads) fields_group_kernel(EngineView 
     }
     if (!site) return;
 #pragma unroll
-    for (int g = 0; g < kFieldGroup; ++g)
+    for (int g = 0; g < G; ++g)
         if (g < group) fields[static_cast<size_t>(k0 + g) * field_stride + i] = sum[g];
 }
 
@@ -574,10 +575,17 @@ void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream) {
 void compute_fields(const EngineView& v, const int8_t* spins, int64_t spin_stride, double* fields,
                     int64_t field_stride, double* energies, int count, cudaStream_t stream) {
     if (count <= 0) return;
-    if (!v.csr && count > 1) {
-        const dim3 grid(static_cast<unsigned>((v.n + kFieldThreads - 1) / kFieldThreads),
-                        static_cast<unsigned>((count + kFieldGroup - 1) / kFieldGroup));
-        fields_group_kernel<<<grid, kFieldThreads, 0, stream>>>(v, spins, spin_stride, fields, field_stride, count);
+    if (!v.csr && count >= 64 && v.n >= 1024) {  // many configurations of a large system
+        constexpr int G = 32, TILE = 64, THREADS = 64;
+        const dim3 grid(static_cast<unsigned>((v.n + THREADS - 1) / THREADS), static_cast<unsigned>((count + G - 1) / G));
+        fields_group_kernel<G, TILE, THREADS><<<grid, THREADS, 0, stream>>>(v, spins, spin_stride, fields, field_stride,
+                                                                             count);
+        check_cuda(cudaGetLastError(), "fields_group_kernel");
+    } else if (!v.csr && count > 1) {
+        constexpr int G = 8, TILE = 256, THREADS = 128;
+        const dim3 grid(static_cast<unsigned>((v.n + THREADS - 1) / THREADS), static_cast<unsigned>((count + G - 1) / G));
+        fields_group_kernel<G, TILE, THREADS><<<grid, THREADS, 0, stream>>>(v, spins, spin_stride, fields, field_stride,
+                                                                             count);
         check_cuda(cudaGetLastError(), "fields_group_kernel");
     } else {
         const dim3 grid(static_cast<unsigned>((v.n + 127) / 128), static_cast<unsigned>(count));

@@ -108,3 +108,17 @@ def test_coincident_sites_rejected():
     g = Geometry(np.zeros((2, 3)), np.tile([0.0, 0.0, 1.0], (2, 1)), (0, 0, 0), False)
     with pytest.raises(InvalidArgument, match="Coincident dipole sites"):
         System(g).couplings()
+
+
+def test_local_fields_many_configurations_bitwise(oracle):
+    """70 configurations of an 1100-site system take the 32-configurations-per-block field
+    kernel (groups of 32, 32 and 6); every field and energy equals the oracle's sequential sum."""
+    g = Geometry.simple_cubic(11, 10, 10, periodic=True)
+    g.axes = random_axes(g.size(), 77)
+    s = System(g, 1.0, 0.0)
+    rng = np.random.default_rng(5)
+    spins = rng.choice(np.array([-1, 1], dtype=np.int8), size=(70, s.size()))
+    f, e = s.local_fields(spins)
+    fo, eo = oracle.local_fields(s, spins)
+    assert same_double(f, fo)
+    assert same_double(e, eo)
