@@ -316,18 +316,27 @@ typedef struct wlg_autotune_report {
     int32_t epochs_per_graph;    /* chosen epochs per CUDA-graph replay                        */
     double ms_per_epoch;         /* device time per epoch of the chosen shape                  */
     uint64_t trials;             /* candidate shapes timed                                     */
+    int32_t staging_ring;        /* chosen staging depth of the split sweep (0: not used)      */
+    int32_t pad;
 } wlg_autotune_report;
 
 /* Launch-shape autotuner: times candidate shapes (walkers per CTA 1-8 for the generic sweep,
- * epochs per graph 4-64) on trial_epochs real epochs each through the product path and keeps
- * the fastest.  The shape never changes results, so the trial epochs count as epochs of the
- * run.  The exchange interval, which changes trajectories, is not tuned.  No counterpart in
- * the reference. */
+ * epochs per graph 4-64, the split sweep's staging depth of 16 or 32 draws with their J rows
+ * where both fit in shared memory) on trial_epochs real epochs each through the product path
+ * and keeps the fastest.  The shape never changes results, so the trial epochs count as epochs
+ * of the run.  The exchange interval, which changes trajectories, is not tuned.  No
+ * counterpart in the reference. */
 wlg_status wlg_engine_autotune(wlg_engine* engine, uint64_t trial_epochs, wlg_autotune_report* out);
 /* Launch shape: walkers per CTA of the sweep kernel (1-8) and epochs per CUDA-graph
  * replay (>= 1); 0 leaves a value unchanged.  No counterpart in the reference. */
 wlg_status wlg_engine_set_launch(wlg_engine* engine, int32_t walkers_per_block,
                                  int32_t epochs_per_graph);
+/* The split sweep's staging ring (dense systems up to 1024 sites without pilot statistics or
+ * the Nalivaiko mask): entries = 16 or 32 draws, each with its site's J row copied into shared
+ * memory ahead of the walker; 0 restores 16.  WLG_ERR_INVALID_ARGUMENT when the engine's sweep
+ * has no such ring or it does not fit.  Results do not depend on it.  No counterpart in the
+ * reference. */
+wlg_status wlg_engine_set_staging_ring(wlg_engine* engine, int32_t entries);
 /* Single-window runs of small dense systems (one window, FP64 couplings, at most 32 sites
  * and 4 walkers, no pilot statistics or Nalivaiko mask) run many epochs per launch in one
  * CTA; this is the default for such engines.  enabled = 0 selects the per-epoch kernels

@@ -168,6 +168,8 @@ class wlg_autotune_report(C.Structure):
         ("epochs_per_graph", C.c_int32),
         ("ms_per_epoch", C.c_double),
         ("trials", C.c_uint64),
+        ("staging_ring", C.c_int32),
+        ("pad", C.c_int32),
     ]
 
 
@@ -277,6 +279,7 @@ SIGNATURES = {
     "wlg_engine_create_from_couplings": (_i32, [P(wlg_couplings), P(wlg_run_config), P(_vp)]),
     "wlg_engine_destroy": (None, [_vp]),
     "wlg_engine_inject_wait_timeout": (_i32, [_vp]),
+    "wlg_engine_set_staging_ring": (_i32, [_vp, _i32]),
     "wlg_engine_run": (_i32, [_vp, P(wlg_run_totals)]),
     "wlg_engine_run_epochs": (_i32, [_vp, _u64, P(_u64), P(_i32)]),
     "wlg_engine_totals": (_i32, [_vp, P(wlg_run_totals)]),

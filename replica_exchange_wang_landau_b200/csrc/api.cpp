@@ -336,6 +336,11 @@ wlg_status wlg_engine_stitch(wlg_engine* engine, int32_t complete_range, double*
     });
 }
 
+wlg_status wlg_engine_set_staging_ring(wlg_engine* engine, int32_t entries) {
+    WLG_ENGINE_GUARD(engine)
+    return guarded([&] { engine->impl->set_staging_ring(entries); });
+}
+
 wlg_status wlg_engine_inject_wait_timeout(wlg_engine* engine) {
     WLG_ENGINE_GUARD(engine)
     return guarded([&] { engine->impl->inject_wait_timeout(); });

@@ -310,6 +310,7 @@ struct EngineView {
     const float* ell_val32;        // FP32 couplings (FP32 runs)
     int32_t ell_width;             // 32, 64, 128 or 256; 0 when not built
     int32_t spins_global;          // the generic sweep and the initialisation read spins from HBM
+    int32_t split_ring_log;        // split sweep: log2 of its draw / J-row staging ring (4 or 5; 0 = 4)
     Grid grid;
     int32_t walkers;
     int32_t walkers_per_window;

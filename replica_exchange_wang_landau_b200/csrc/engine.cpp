@@ -881,32 +881,67 @@ void Engine::autotune(uint64_t trial_epochs, wlg_autotune_report* out) {
     const int* wpbs = generic ? wpbs_generic : wpbs_dense;
     const int n_wpb = generic ? 4 : 1;
     const int epgs[] = {4, 8, 16, 32, 64};
+    // the split sweep's staging depth (16 or 32 draws with their J rows) where it serves the engine
+    std::vector<int> rings;
+    for (int rl : split_ring_logs(view_)) rings.push_back(1 << rl);
+    if (rings.empty()) rings.push_back(0);
     wlg_autotune_report r{};
     double best = std::numeric_limits<double>::infinity();
-    int best_wpb = walkers_per_block, best_epg = epochs_per_graph;
-    for (int a = 0; a < n_wpb && !done_; ++a) {
-        for (int epg : epgs) {
-            if (done_) break;
-            set_launch(wpbs[a], epg);
-            wlg_epoch_timing t{};
-            time_run(static_cast<uint64_t>(epg), &t);  // builds and warms the graph
-            const uint64_t rounds = std::max<uint64_t>(1, (trial_epochs + epg - 1) / epg);
-            time_run(rounds * epg, &t);
-            ++r.trials;
-            if (t.epochs == 0) continue;
-            const double per_epoch = t.total_ms / static_cast<double>(t.epochs);
-            if (per_epoch < best) {
-                best = per_epoch;
-                best_wpb = wpbs[a];
-                best_epg = epg;
+    int best_wpb = walkers_per_block, best_epg = epochs_per_graph, best_ring = staging_ring();
+    for (int ring : rings) {
+        if (ring) set_staging_ring(ring);
+        for (int a = 0; a < n_wpb && !done_; ++a) {
+            for (int epg : epgs) {
+                if (done_) break;
+                set_launch(wpbs[a], epg);
+                wlg_epoch_timing t{};
+                time_run(static_cast<uint64_t>(epg), &t);  // builds and warms the graph
+                const uint64_t rounds = std::max<uint64_t>(1, (trial_epochs + epg - 1) / epg);
+                time_run(rounds * epg, &t);
+                ++r.trials;
+                if (t.epochs == 0) continue;
+                const double per_epoch = t.total_ms / static_cast<double>(t.epochs);
+                if (per_epoch < best) {
+                    best = per_epoch;
+                    best_wpb = wpbs[a];
+                    best_epg = epg;
+                    best_ring = ring ? ring : staging_ring();
+                }
             }
         }
     }
+    if (rings.front() != 0) set_staging_ring(best_ring);
     set_launch(best_wpb, best_epg);
     r.walkers_per_block = best_wpb;
     r.epochs_per_graph = best_epg;
     r.ms_per_epoch = std::isfinite(best) ? best : 0.0;
+    r.staging_ring = staging_ring();
     if (out) *out = r;
+}
+
+void Engine::set_staging_ring(int entries) {
+    int rl = 0;
+    if (entries == 16) rl = 4;
+    else if (entries == 32) rl = 5;
+    else if (entries != 0) throw WlgError(WLG_ERR_INVALID_ARGUMENT, "The staging ring holds 16 or 32 draws");
+    if (rl != 0) {
+        const std::vector<int> ok = split_ring_logs(view_);
+        if (std::find(ok.begin(), ok.end(), rl) == ok.end())
+            throw WlgError(WLG_ERR_INVALID_ARGUMENT,
+                           "This engine's sweep has no staging ring of " + std::to_string(entries) + " draws");
+    }
+    if (rl == view_.split_ring_log) return;
+    view_.split_ring_log = rl;
+    // the epoch graph holds the kernels' arguments by value: capture it again
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    graph_exec_ = nullptr;
+    graph_ = nullptr;
+}
+
+int Engine::staging_ring() const {
+    if (split_ring_logs(view_).empty()) return 0;
+    return 1 << (view_.split_ring_log == 5 ? 5 : 4);
 }
 
 void Engine::totals(wlg_run_totals* out) {

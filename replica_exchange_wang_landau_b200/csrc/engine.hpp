@@ -186,6 +186,9 @@ void launch_init(const EngineView& v, const InitArgs& a, int walkers_per_block, 
 void launch_walk(const EngineView& v, const WalkArgs& a, int walkers_per_block, cudaStream_t stream);
 // sweep.cu: the dense sweep; false when the walker does not fit the shared-memory ring.
 bool launch_sweep_dense(const EngineView& v, const WalkArgs& a, cudaStream_t stream);
+// The split sweep's possible staging depths for this engine (log2 of the draw / J-row ring);
+// empty when the split sweep does not serve it.
+std::vector<int> split_ring_logs(const EngineView& v);
 bool launch_sweep_csr(const EngineView& v, const WalkArgs& a, int walkers_per_block, cudaStream_t stream);
 // sweep_window.cu: whole epochs of a single-window run of a dense FP64 system of at most 32
 // sites and 4 walkers, without pilot statistics or the Nalivaiko mask, in one launch
@@ -268,6 +271,9 @@ class Engine {
     void time_run(uint64_t epochs, wlg_epoch_timing* out);
     void autotune(uint64_t trial_epochs, wlg_autotune_report* out);
     void set_launch(int walkers_per_block, int epochs_per_graph);
+    // the split sweep's staging ring (draws with their J rows): 16 or 32 entries, 0 = 16
+    void set_staging_ring(int entries);
+    int staging_ring() const;
     // Failure injection for tests: from the next epoch on, the draw producers of the split and
     // single-window sweeps publish nothing, so every walker's bounded wait runs out.
     void inject_wait_timeout();

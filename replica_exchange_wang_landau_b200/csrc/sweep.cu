@@ -497,15 +497,17 @@ __global__ void __launch_bounds__(32, 1) sweep_dense_kernel(EngineView v, WalkAr
 
 constexpr uint32_t kProducerPolls = 1u << 24;
 constexpr int kDrawBatch = 4;  // draws per producer batch (one barrier per batch)
-// Ring of 16 draws: the walker reads up to draw hq+4 while it still holds the row of draw
+// The ring holds 2^kRL draws with their J rows (the staging depth; the autotuner chooses 4
+// or 5).  At least 16: the walker reads up to draw hq+4 while it still holds the row of draw
 // hq-1 or hq-2, and the producer must be able to complete the batch holding draw hq+4.
-constexpr int kRingLog = 4;
+constexpr int kMinRingLog = 4;
+constexpr int kMaxRingLog = 5;
 
 struct SplitLayout {
     size_t ring, bars, lnu, rs, site, hd, ctl, base, total;
 };
-__host__ __device__ inline SplitLayout split_layout(int ld, int mwb, size_t jbytes) {
-    constexpr size_t q = size_t{1} << kRingLog;
+__host__ __device__ inline SplitLayout split_layout(int ld, int mwb, size_t jbytes, int ring_log) {
+    const size_t q = size_t{1} << ring_log;
     SplitLayout L;
     size_t at = 0;
     L.ring = at; at += q * round16(static_cast<size_t>(ld) * jbytes);
@@ -565,11 +567,11 @@ __device__ __forceinline__ double2 coupling_pair(const typename CouplingType<kPr
     }
 }
 
-template <int kChunks, bool kPow2, int kPrec>
+template <int kChunks, bool kPow2, int kPrec, int kRL>
 __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, WalkArgs a) {
     using JT = typename CouplingType<kPrec>::T;
     extern __shared__ __align__(128) unsigned char smem[];
-    constexpr int qlog = kRingLog;
+    constexpr int qlog = kRL;
     constexpr uint32_t qm = (1u << qlog) - 1u;
     constexpr int blog = qlog - 2;  // log2 of the number of batch barriers (kDrawBatch == 4)
     constexpr uint32_t bm = (1u << blog) - 1u;
@@ -580,7 +582,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
     if (a.epoch_mode && *reinterpret_cast<volatile int32_t*>(&ctl->done)) return;
 
     const int ld = v.ld;
-    const SplitLayout SL = split_layout(ld, v.max_window_bins, sizeof(JT));
+    const SplitLayout SL = split_layout(ld, v.max_window_bins, sizeof(JT), kRL);
     const SmemLayout L = smem_layout(ld, v.max_window_bins, true, false);
     const size_t row_stride = round16(static_cast<size_t>(ld) * sizeof(JT)) / sizeof(JT);  // elements
     const JT* ring = reinterpret_cast<const JT*>(smem + SL.ring);
@@ -1037,49 +1039,70 @@ SweepFn sweep_fn() {
 
 }  // namespace
 
-template <int K, bool kPow2, int kPrec>
+template <int K, bool kPow2, int kPrec, int kRL>
 SweepFn split_fn() {
     static bool configured = false;
     if (!configured) {
-        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_dense_split_kernel<K, kPow2, kPrec>),
+        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_dense_split_kernel<K, kPow2, kPrec, kRL>),
                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
                    "cudaFuncSetAttribute");
         configured = true;
     }
-    return &sweep_dense_split_kernel<K, kPow2, kPrec>;
+    return &sweep_dense_split_kernel<K, kPow2, kPrec, kRL>;
 }
 
 // Chunks of 64 couplings per lane pass, rounded up to a power of two (unused chunks are
 // masked off), for ld <= 1024.
-template <bool kPow2, int kPrec>
+template <bool kPow2, int kPrec, int kRL>
 SweepFn pick_split_chunks(int ld) {
     const int chunks = (ld + 63) / 64;
-    if (chunks <= 1) return split_fn<1, kPow2, kPrec>();
-    if (chunks <= 2) return split_fn<2, kPow2, kPrec>();
-    if (chunks <= 4) return split_fn<4, kPow2, kPrec>();
-    if (chunks <= 8) return split_fn<8, kPow2, kPrec>();
-    if (chunks <= 16) return split_fn<16, kPow2, kPrec>();
+    if (chunks <= 1) return split_fn<1, kPow2, kPrec, kRL>();
+    if (chunks <= 2) return split_fn<2, kPow2, kPrec, kRL>();
+    if (chunks <= 4) return split_fn<4, kPow2, kPrec, kRL>();
+    if (chunks <= 8) return split_fn<8, kPow2, kPrec, kRL>();
+    if (chunks <= 16) return split_fn<16, kPow2, kPrec, kRL>();
     return nullptr;
 }
 
-template <int kPrec>
+template <int kPrec, int kRL>
 SweepFn pick_split_precision(int ld, bool pow2_width) {
-    return pow2_width ? pick_split_chunks<true, kPrec>(ld) : pick_split_chunks<false, kPrec>(ld);
+    return pow2_width ? pick_split_chunks<true, kPrec, kRL>(ld) : pick_split_chunks<false, kPrec, kRL>(ld);
 }
 
-// The split sweep for dense couplings with ld <= 1024.
-SweepFn pick_split(int ld, bool pow2_width, int precision) {
-    if (precision == WLG_PRECISION_FP32) return pick_split_precision<WLG_PRECISION_FP32>(ld, pow2_width);
-    if (precision == WLG_PRECISION_BF16) return pick_split_precision<WLG_PRECISION_BF16>(ld, pow2_width);
-    return pick_split_precision<WLG_PRECISION_FP64>(ld, pow2_width);
+template <int kRL>
+SweepFn pick_split_ring(int ld, bool pow2_width, int precision) {
+    if (precision == WLG_PRECISION_FP32) return pick_split_precision<WLG_PRECISION_FP32, kRL>(ld, pow2_width);
+    if (precision == WLG_PRECISION_BF16) return pick_split_precision<WLG_PRECISION_BF16, kRL>(ld, pow2_width);
+    return pick_split_precision<WLG_PRECISION_FP64, kRL>(ld, pow2_width);
+}
+
+// The split sweep for dense couplings with ld <= 1024, with a staging ring of 2^ring_log draws.
+SweepFn pick_split(int ld, bool pow2_width, int precision, int ring_log) {
+    return ring_log == kMaxRingLog ? pick_split_ring<kMaxRingLog>(ld, pow2_width, precision)
+                                   : pick_split_ring<kMinRingLog>(ld, pow2_width, precision);
+}
+
+// Staging depths (log2 of the ring) the split sweep can run for this engine: those whose
+// ring and window slice fit in one CTA's shared memory; empty when the split sweep does not
+// serve it.
+std::vector<int> split_ring_logs(const EngineView& v) {
+    std::vector<int> out;
+    const bool features = v.p.collect || v.p.nalivaiko;
+    if (features || v.ld > 1024) return out;
+    const size_t jbytes = v.precision == WLG_PRECISION_FP64 ? 8 : v.precision == WLG_PRECISION_FP32 ? 4 : 2;
+    for (int rl = kMinRingLog; rl <= kMaxRingLog; ++rl)
+        if (split_layout(v.ld, v.max_window_bins, jbytes, rl).total <= 227 * 1024) out.push_back(rl);
+    return out;
 }
 
 bool launch_sweep_dense(const EngineView& v, const WalkArgs& a, cudaStream_t stream) {
     const bool features = v.p.collect || v.p.nalivaiko;
     const size_t jbytes = v.precision == WLG_PRECISION_FP64 ? 8 : v.precision == WLG_PRECISION_FP32 ? 4 : 2;
     if (!features && v.ld <= 1024) {  // the split sweep
-        SweepFn fn = pick_split(v.ld, v.grid.pow2_width != 0, v.precision);
-        const size_t split_bytes = split_layout(v.ld, v.max_window_bins, jbytes).total;
+        int rl = v.split_ring_log == kMaxRingLog ? kMaxRingLog : kMinRingLog;
+        if (split_layout(v.ld, v.max_window_bins, jbytes, rl).total > 227 * 1024) rl = kMinRingLog;
+        SweepFn fn = pick_split(v.ld, v.grid.pow2_width != 0, v.precision, rl);
+        const size_t split_bytes = split_layout(v.ld, v.max_window_bins, jbytes, rl).total;
         if (fn && split_bytes <= 227 * 1024) {
             fn<<<static_cast<unsigned>(a.count), 64, split_bytes, stream>>>(v, a);
             check_cuda(cudaGetLastError(), "sweep_dense_split_kernel");

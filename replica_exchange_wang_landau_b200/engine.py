@@ -638,6 +638,10 @@ class Engine:
         fn = self._lib.wlg_engine_warm_start_continue if continue_schedule else self._lib.wlg_engine_warm_start
         _check(fn(self._h, _dptr(lg), float(factor)))
 
+    def set_staging_ring(self, entries: int) -> None:
+        """The split sweep's staging ring: 16 or 32 draws with their J rows (0 = 16)."""
+        _check(self._lib.wlg_engine_set_staging_ring(self._h, int(entries)))
+
     def inject_wait_timeout(self) -> None:
         """Failure injection for tests: the draw producers of the split and single-window sweeps
         publish nothing from the next epoch on, so the walkers' bounded waits run out and the

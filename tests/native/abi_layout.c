@@ -51,7 +51,7 @@ int main(void) {
     F(wlg_precision_report, resynced); F(wlg_precision_report, deferred); F(wlg_precision_report, bin_changes);
     F(wlg_precision_report, max_field_drift); F(wlg_precision_report, max_energy_drift);
     S(wlg_autotune_report); F(wlg_autotune_report, walkers_per_block); F(wlg_autotune_report, epochs_per_graph);
-    F(wlg_autotune_report, ms_per_epoch); F(wlg_autotune_report, trials);
+    F(wlg_autotune_report, ms_per_epoch); F(wlg_autotune_report, trials); F(wlg_autotune_report, staging_ring); F(wlg_autotune_report, pad);
     S(wlg_fragment_view); F(wlg_fragment_view, window_begin); F(wlg_fragment_view, window_end);
     F(wlg_fragment_view, log_g); F(wlg_fragment_view, histogram); F(wlg_fragment_view, standard_error);
     F(wlg_fragment_view, valid);

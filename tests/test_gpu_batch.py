@@ -74,6 +74,38 @@ def test_autotune_keeps_results(cutoff):
         r = e.autotune(4)
         assert r["epochs_per_graph"] in (4, 8, 16, 32, 64) and 1 <= r["walkers_per_block"] <= 8
         assert r["trials"] >= 5 and r["ms_per_epoch"] > 0
+        if cutoff > 0:
+            assert r["staging_ring"] == 0  # the CSR sweep has no staging ring
+        else:  # the dense engine runs the split sweep: both staging depths are candidates
+            assert r["staging_ring"] in (16, 32) and r["trials"] >= 10
         e.run()
         for w in range(4):
             assert snapshots_equal(e.snapshot(w), plain[w]) == []
+
+
+def test_staging_ring_keeps_results(oracle):
+    """The split sweep with a 32-draw staging ring, switched between epochs, runs bit for bit
+    like the oracle (512 sites, 3 windows, 1/t stage reached)."""
+    from helpers import results_equal
+    s = System(simple_cubic_random(8, 8, 8, seed=18, periodic=True), 1.0, 0.0)
+    c = RunConfig(emin=-228.5, emax=228.0, bin_width=0.5, windows=3, walkers=2, seed=19, exchange_interval_mcs=1)
+    c.wl.final_factor = 1e-2
+    c.check_interval_mcs = 5
+    c.max_mcs = 300
+    c.resolve_mcs(s.size())
+    with Engine(s, c) as e:
+        e.set_staging_ring(32)
+        e.run_epochs(100)
+        e.set_staging_ring(16)
+        e.run_epochs(50)
+        e.set_staging_ring(32)
+        e.run()
+        got = e.result()
+        with pytest.raises(Exception):
+            e.set_staging_ring(24)
+    assert results_equal(got, oracle.run_rewl(s, c)) == []
+    cs = System(simple_cubic_random(4, 4, 4, seed=3, periodic=True), 1.0, 1.8)
+    cc = RunConfig(emin=-60, emax=60, bin_width=0.5, windows=1, walkers=1, seed=9).resolve_mcs(64)
+    with Engine(cs, cc) as e:
+        with pytest.raises(Exception):
+            e.set_staging_ring(32)  # the CSR sweep has no staging ring
