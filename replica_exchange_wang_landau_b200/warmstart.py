@@ -178,9 +178,12 @@ def plain_dos(system: System, emin: float, emax: float, width: float, seed: int 
     return DosSample(system, emin, emax, width, np.asarray(frag.log_g, np.float64), np.asarray(frag.valid, bool))
 
 
-def plain_dos_many(specs: Sequence[tuple], final_factor: float = 1e-4, walkers: int = 2) -> list:
+def plain_dos_many(specs: Sequence[tuple], final_factor: float = 1e-4, walkers: int = 2,
+                   epoch_attempts: Optional[int] = None) -> list:
     """plain_dos for many (system, emin, emax, width, seed) at once: the engines run side by
-    side in one batch (one CUDA-graph launch advances all of them)."""
+    side in one batch (one CUDA-graph launch advances all of them).  epoch_attempts: attempts
+    per walker per epoch (default 10 MCS; a fixed count keeps engines of different sizes at the
+    same pace in the batch)."""
     from .engine import Batch
     engines = []
     try:
@@ -188,6 +191,9 @@ def plain_dos_many(specs: Sequence[tuple], final_factor: float = 1e-4, walkers: 
             c = RunConfig(emin=emin, emax=emax, bin_width=width, windows=1, walkers=walkers, seed=seed)
             c.wl = WlParameters(0.8, 100, final_factor, 1000, 0, True)
             c.exchange_interval_mcs = 10.0
+            if epoch_attempts:
+                c.exchange_interval_uses_mcs = False
+                c.exchange_interval_attempts = int(epoch_attempts)
             c.max_mcs = 1e7
             c.resolve_mcs(system.size())
             engines.append(Engine(system, c))
@@ -336,13 +342,21 @@ def accuracy_error(log_g: np.ndarray, valid: np.ndarray, judge_log_g: np.ndarray
     return float(np.max(np.abs(d - d.mean())))
 
 
+EPOCH_ATTEMPTS = 8192  # attempts per walker per epoch of the learned configuration's runs
+
+
 def single_window_config(emin: float, emax: float, width: float, n: int, seed: int, final_factor: float,
                          walkers: int = 2, precision: str = "fp64") -> RunConfig:
-    """One window of `walkers` walkers, 1/t Wang-Landau to final_factor, exchange interval 10 MCS
-    (the epoch), FP64 recompute once per epoch for FP32 / BF16 couplings."""
+    """One window of `walkers` walkers, 1/t Wang-Landau to final_factor.  The epoch (with one
+    window only the interval between checks and launches) is EPOCH_ATTEMPTS attempts whatever
+    N is, so that engines of different sizes advanced together in one batch make the same
+    number of attempts per launch: the attempts a run needs do not grow with N (the 1/t stage
+    takes about bins / ln f of them), so epochs of a fixed number of MCS would hold the small
+    systems back to the pace of the largest.  FP64 recompute every 10 MCS for FP32 / BF16."""
     c = RunConfig(emin=emin, emax=emax, bin_width=width, windows=1, walkers=walkers, seed=seed)
     c.wl = WlParameters(0.8, 100, final_factor, 1000, 0, True)
-    c.exchange_interval_mcs = 10.0
+    c.exchange_interval_uses_mcs = False
+    c.exchange_interval_attempts = EPOCH_ATTEMPTS
     c.max_mcs = 0.0
     c.coupling_precision = precision
     c.recompute_interval_mcs = 10.0
