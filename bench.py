@@ -553,7 +553,7 @@ def csr_batched_line(epochs: int = 40, pilot_mcs: float = 20.0, with_cpu_baselin
 
 
 def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e-3, judge_factor: float = 3e-6,
-                               sequential_sample: int = 8, cpu_sample: int = 2) -> dict:
+                               sequential_sample: int = 8, cpu_sample: int = 8) -> dict:
     """The learned configuration, time to accuracy: 256 generated dilute systems (N uniform in
     64..1024, random sequential addition at density 0.3-0.8, random-sphere axes; one window of 2
     walkers over about +-4 sigma in 200 bins).  The warm-start network is trained on the GPU on
@@ -570,8 +570,8 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
     Time to ln f <= 1e-8 of each arm is extrapolated from its measured attempts per walker per
     second (1/t: active bins / 1e-8 attempts per walker, less the continued schedule's offset).
     The reference's run_rewl (compiled from its sources, 2 walkers on 2 host threads) is timed
-    on `cpu_sample` held-out systems; its time to the tolerance is the plain runs' attempts per
-    walker over its rate, 56 systems on all host cores."""
+    on the systems the sequential arm timed; its time to the tolerance is each plain run's
+    attempts per walker over the reference's rate on that system, 56 systems on all host cores."""
     from replica_exchange_wang_landau_b200.engine import Engine
     from replica_exchange_wang_landau_b200.warmstart import (EPOCH_ATTEMPTS, WarmStartModel, batch_to_accuracy,
                                                              dilute_instance, engine_to_accuracy, plain_dos_many,
@@ -657,14 +657,15 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
         "seconds_90pct_scaled": per_system * np.ceil(0.9 * len(held)) if per_system else None,
         "median_attempts_per_walker": float(np.median([r["attempts_per_walker"] for r in ok])) if ok else None,
         "ln_f_1e-8_s_extrapolated_all_56": float(np.mean([r["ln_f_1e-8_s"] for r in seq])) * len(held)}
-    # the reference on the host: its rate on held-out systems, applied to the plain attempts
+    # the reference on the host: its rate on each system the sequential arm timed, applied to the
+    # attempts that system's plain run needed; 56 systems over the host cores, two threads each
     cpu = None
     try:
         from oracle.oracle import Reference
         ref = Reference()
         threads = ref.set_threads(2)
-        rates = []
-        for k in range(cpu_sample):
+        seconds, rates, ln_f = [], [], []
+        for k in range(min(cpu_sample, len(seq))):
             s, lo, hi, w = held[k]
             c = single_window_config(lo, hi, w, s.size(), 20_000 + k, 1e-8)
             c.max_mcs = 2000.0
@@ -672,16 +673,21 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
             c.resolve_mcs(s.size())
             t1 = time.perf_counter()
             rr = ref.run_rewl(s, c)
-            rates.append(rr.attempted / 2 / (time.perf_counter() - t1))
-        rate = float(np.mean(rates))
-        need = arms["plain_sequential"]["median_attempts_per_walker"]
+            rate = rr.attempted / 2 / (time.perf_counter() - t1)
+            rates.append(rate)
+            if seq[k]["attempts_per_walker"]:
+                seconds.append(seq[k]["attempts_per_walker"] / rate)
+            ln_f.append(seq[k]["active_bins"] / 1e-8 / rate)
         parallel = max(1, (os.cpu_count() or 2) // 2)
-        cpu = {"attempts_per_walker_per_s": rate, "threads_per_system": threads, "systems_in_parallel": parallel,
-               "seconds_all_56_extrapolated": need / rate * len(held) / parallel if need else None,
-               "ln_f_1e-8_s_all_56_extrapolated": float(np.mean([r["active_bins"] for r in seq])) / 1e-8 / rate *
-               len(held) / parallel,
-               "sample": f"reference run_rewl (oracle/_ref) on {cpu_sample} held-out systems, 2 walkers on "
-                         f"{threads} threads, 2000 MCS"}
+        cpu = {"attempts_per_walker_per_s": {"min": min(rates), "mean": float(np.mean(rates)), "max": max(rates)},
+               "threads_per_system": threads, "systems_in_parallel": parallel,
+               "seconds_all_56_extrapolated": float(np.mean(seconds)) * len(held) / parallel if seconds else None,
+               "seconds_90pct_extrapolated": float(np.mean(seconds)) * np.ceil(0.9 * len(held)) / parallel
+               if seconds else None,
+               "ln_f_1e-8_s_all_56_extrapolated": float(np.mean(ln_f)) * len(held) / parallel,
+               "sample": f"reference run_rewl (oracle/_ref), 2 walkers on {threads} threads, 2000 MCS, on the "
+                         f"{len(rates)} systems the sequential arm timed; each system's time = the plain run's "
+                         f"attempts per walker / the reference's rate on it"}
     except Exception as exc:
         cpu = {"error": str(exc)}
     # ratios on the time until 90% of the held-out systems met the tolerance (robust to a system
