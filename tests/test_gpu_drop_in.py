@@ -83,3 +83,27 @@ def test_drop_in_csr_adaptive_windows(tmp_path):
                                     "--adaptive-pilot-mcs", "30", "--exchange-interval-mcs", "1", "--max-mcs", "100",
                                     "--seed", "9"])
     assert rc == 2 and "run_window_0.csv" in files
+
+
+def test_drop_in_single_walker_checkpoint_and_resume(tmp_path):
+    # one window of one walker writes the reference's WLCHKP3 checkpoint (src/parallel.cpp:522-525);
+    # a second run with a higher max-mcs restores it (src/parallel.cpp:354-360) and continues
+    if not (WL_RUN.exists() and WL_RUN_B200.exists()):
+        pytest.skip("oracle/_ref/wl_run and wl_run_b200 were not built")
+    base = ["--nx", "3", "--ny", "2", "--nz", "2", "--periodic", "false", "--emin", "-30", "--emax", "30",
+            "--bin-width", "0.25", "--windows", "1", "--walkers", "1", "--seed", "8", "--checkpoint-interval-mcs", "50"]
+    outputs = {}
+    for name, binary in (("cpu", WL_RUN), ("gpu", WL_RUN_B200)):
+        out = tmp_path / name
+        chk = out / "run.chk"
+        first = _run(binary, base + ["--checkpoint", str(chk), "--max-mcs", "200"], out)
+        second = _run(binary, base + ["--checkpoint", str(chk), "--max-mcs", "400"], out)
+        outputs[name] = (first, second)
+    for k in (0, 1):
+        rc_a, out_a, files_a, err_a = outputs["cpu"][k]
+        rc_b, out_b, files_b, err_b = outputs["gpu"][k]
+        assert rc_a == rc_b == 2, (err_a, err_b)
+        assert out_b == out_a
+        assert sorted(files_b) == sorted(files_a) and "run.chk" in files_a
+        for name in files_a:
+            assert files_b[name] == files_a[name], name
