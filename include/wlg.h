@@ -368,8 +368,9 @@ wlg_status wlg_engine_warm_start(wlg_engine* engine, const double* log_g, double
  * usual and then enters the 1/t stage at once from the factor reached, counting
  * round(active / factor) - attempted attempts as already made: from then on
  * f = active / (attempted + offset) (update_inverse_time_factor, src/wang_landau.cpp:309-315,
- * with the offset added), so f never rises above the warm start's and falls as 1/t.  An
- * extension with no counterpart in the reference. */
+ * with the offset added): f starts from the factor reached and falls as 1/t, rising, as under
+ * the reference's rule, only when the walker finds a new bin.  An extension with no
+ * counterpart in the reference. */
 wlg_status wlg_engine_warm_start_continue(wlg_engine* engine, const double* log_g, double factor);
 uint64_t wlg_engine_walkers(const wlg_engine* engine);
 uint64_t wlg_engine_bins(const wlg_engine* engine);

@@ -301,8 +301,8 @@ class Engine {
     void swap(uint64_t left, uint64_t right);
     void precision_report(wlg_precision_report* out);
     // continue_schedule: the first covered check enters the 1/t stage at the factor reached and
-    // counts round(active / factor) attempts as made (f = active / (attempted + offset)), so
-    // the factor never rises above the warm start's; false keeps the reference's rule.
+    // counts round(active / factor) attempts as made (f = active / (attempted + offset)), so the
+    // factor starts where the warm start left it; false keeps the reference's rule.
     void warm_start(const double* log_g, double factor, bool continue_schedule = false);
     // every walker's state, the control block and the recompute schedule (multi-walker
     // checkpoint; the reference checkpoints single-walker runs only)

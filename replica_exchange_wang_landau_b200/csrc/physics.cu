@@ -303,8 +303,9 @@ __global__ void fields_kernel(EngineView v, const int8_t* __restrict__ spins, in
 // broadcast (a double2) per two terms.  Every field is still summed sequentially over j with
 // the reference's operations (sum += J(i, j) * s_j, no contraction), so the result is the one
 // of fields_kernel whatever G is.  A block reads its sites' columns of J once for G
-// configurations: G = 8 keeps many blocks in flight for small counts; G = 32 reads J four times
-// less (the FP64 recompute of 256 walkers at N = 2458 read the 48 MB J 32 times with G = 8).
+// configurations.  G = 8 is used: G = 32 (64 threads, 128 registers) reads J four times less but
+// leaves a quarter of the warps, and the FP64 recompute of 256 walkers at N = 2458 took 0.56 ms
+// with it against 0.43 ms with G = 8.
 constexpr int kFieldPrefetch = 8;   // rows of J in flight per thread
 template <int G, int TILE, int THREADS>
 __global__ void __launch_bounds__(THREADS) fields_group_kernel(EngineView v, const int8_t* __restrict__ spins,
@@ -575,13 +576,7 @@ void build_couplings(DeviceSystem& d, int precision, cudaStream_t stream) {
 void compute_fields(const EngineView& v, const int8_t* spins, int64_t spin_stride, double* fields,
                     int64_t field_stride, double* energies, int count, cudaStream_t stream) {
     if (count <= 0) return;
-    if (!v.csr && count >= 64 && v.n >= 1024) {  // many configurations of a large system
-        constexpr int G = 32, TILE = 64, THREADS = 64;
-        const dim3 grid(static_cast<unsigned>((v.n + THREADS - 1) / THREADS), static_cast<unsigned>((count + G - 1) / G));
-        fields_group_kernel<G, TILE, THREADS><<<grid, THREADS, 0, stream>>>(v, spins, spin_stride, fields, field_stride,
-                                                                             count);
-        check_cuda(cudaGetLastError(), "fields_group_kernel");
-    } else if (!v.csr && count > 1) {
+    if (!v.csr && count > 1) {
         constexpr int G = 8, TILE = 256, THREADS = 128;
         const dim3 grid(static_cast<unsigned>((v.n + THREADS - 1) / THREADS), static_cast<unsigned>((count + G - 1) / G));
         fields_group_kernel<G, TILE, THREADS><<<grid, THREADS, 0, stream>>>(v, spins, spin_stride, fields, field_stride,

@@ -1088,7 +1088,7 @@ SweepFn pick_split(int ld, bool pow2_width, int precision, int ring_log) {
 std::vector<int> split_ring_logs(const EngineView& v) {
     std::vector<int> out;
     const bool features = v.p.collect || v.p.nalivaiko;
-    if (features || v.ld > 1024) return out;
+    if (v.csr || features || v.ld > 1024) return out;
     const size_t jbytes = v.precision == WLG_PRECISION_FP64 ? 8 : v.precision == WLG_PRECISION_FP32 ? 4 : 2;
     for (int rl = kMinRingLog; rl <= kMaxRingLog; ++rl)
         if (split_layout(v.ld, v.max_window_bins, jbytes, rl).total <= 227 * 1024) out.push_back(rl);

@@ -111,8 +111,8 @@ def test_coincident_sites_rejected():
 
 
 def test_local_fields_many_configurations_bitwise(oracle):
-    """70 configurations of an 1100-site system take the 32-configurations-per-block field
-    kernel (groups of 32, 32 and 6); every field and energy equals the oracle's sequential sum."""
+    """70 configurations of an 1100-site system in the grouped field kernel (groups of 8 and a
+    last group of 6); every field and energy equals the oracle's sequential sum."""
     g = Geometry.simple_cubic(11, 10, 10, periodic=True)
     g.axes = random_axes(g.size(), 77)
     s = System(g, 1.0, 0.0)

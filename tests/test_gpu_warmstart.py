@@ -134,8 +134,10 @@ WARM_RUNS = {
 @pytest.mark.parametrize("name", list(WARM_RUNS))
 def test_warm_started_run_bitwise(oracle, name, continue_schedule):
     """run_rewl after a warm start at ln f = 1e-3, with the reference's 1/t rule and with the
-    schedule continued (f = active / (attempted + window bins / 1e-3)), bit for bit against the
-    oracle's restatement; the continued schedule's factor never exceeds the start's."""
+    schedule continued (the first covered check enters 1/t from ln f = 5e-4 with f = active /
+    (attempted + offset)), bit for bit against the oracle's restatement.  With the schedule
+    continued the factor stays near the start's: it rises above 5e-4 only as far as new bins
+    raise the active count."""
     make_system, kw = WARM_RUNS[name]
     s = make_system()
     c = RunConfig(**kw)
@@ -152,4 +154,4 @@ def test_warm_started_run_bitwise(oracle, name, continue_schedule):
     assert stages.count(1) + stages.count(2) > 0  # the 1/t stage was reached
     factors = [st["factor"] for st in got.walker_statistics]
     if continue_schedule:
-        assert max(factors) <= 1e-3
+        assert max(factors) <= 2e-3

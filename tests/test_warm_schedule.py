@@ -4,7 +4,8 @@ After a warm start at ln f = f0 the reference's rule (src/wang_landau.cpp:389-40
 the 1/t stage at the first covered check with f = active / attempted, which early in a run is
 far above f0: the small factor of the warm start is thrown away.  Continuing the schedule, the
 check halves f0 and enters the 1/t stage at once, counting round(active / f) - attempted
-attempts as already made, so f = active / (attempted + offset) starts at f0 / 2 and only falls.
+attempts as already made, so f = active / (attempted + offset) starts at f0 / 2 and then falls
+as 1/t, rising only when a new bin raises the active count.
 No reference counterpart; the restatement defines it.
 """
 from __future__ import annotations
