@@ -430,12 +430,13 @@ def batched_instances_line(count: int = 256, epochs: int = 32) -> dict:
     """The batched configuration's scale: `count` dilute random systems (N uniform in 64..1024,
     random sequential addition in a periodic cube at density 0.3-0.8, minimum separation 0.8,
     random-sphere axes; seeded), each one window x 2 walkers over about +-4 sigma of its
-    random-configuration energy distribution in 200 power-of-two bins, advanced together by
-    single graph launches (Batch) and, for comparison, one engine after the other; wall-clock
-    attempts/s of both, host synchronisation included."""
+    random-configuration energy distribution in 200 power-of-two bins, in epochs of 8192 attempts
+    per walker, advanced together by single graph launches (Batch) and, for comparison, one engine
+    after the other; wall-clock attempts/s of both, host synchronisation included."""
     import math
     from replica_exchange_wang_landau_b200.engine import Batch, Engine, RunConfig, System
     from replica_exchange_wang_landau_b200.geometry import random_sequential
+    from replica_exchange_wang_landau_b200.warmstart import EPOCH_ATTEMPTS
     t0 = time.perf_counter()
     engines, sizes = [], []
     try:
@@ -446,6 +447,10 @@ def batched_instances_line(count: int = 256, epochs: int = 32) -> dict:
             sigma = math.sqrt(0.5 * float(np.sum(s.couplings("fp64") ** 2)))
             w = 2.0 ** round(math.log2(8.0 * sigma / 200.0))
             c = RunConfig(emin=-100.0 * w, emax=100.0 * w, bin_width=w, windows=1, walkers=2, seed=k + 1)
+            # epochs of a fixed number of attempts (with one window an epoch only sets when the
+            # check runs and how much a launch advances), so that systems of every size keep pace
+            c.exchange_interval_uses_mcs = False
+            c.exchange_interval_attempts = EPOCH_ATTEMPTS
             c.resolve_mcs(n)
             engines.append(Engine(s, c))
             sizes.append(n)
