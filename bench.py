@@ -557,14 +557,14 @@ def csr_batched_line(epochs: int = 40, pilot_mcs: float = 20.0, with_cpu_baselin
             "max_field_drift": rep["max_field_drift"]}
 
 
-def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e-3, judge_factor: float = 3e-6,
+def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e-3, long_run_factor: float = 3e-6,
                                sequential_sample: int = 8, cpu_sample: int = 8) -> dict:
     """The learned configuration, time to accuracy: 256 generated dilute systems (N uniform in
     64..1024, random sequential addition at density 0.3-0.8, random-sphere axes; one window of 2
     walkers over about +-4 sigma in 200 bins).  The warm-start network is trained on the GPU on
     plain-run DOS curves (ln f = 1e-4) of the first 200; the other 56 are held out.  Each held-out
-    system's judge is a long plain FP64 run of its own (flat start, other seeds, ln f =
-    judge_factor).  Time until max |d log g| <= tolerance against the judge, for:
+    system's reference is a long plain FP64 run of its own (flat start, other seeds, ln f =
+    long_run_factor).  Time until max |d log g| <= tolerance against that run, for:
       plain_sequential -- the plain FP64 GPU form: flat start, one engine at a time (measured on
                           `sequential_sample` systems, the total for 56 scaled from their mean);
       plain_batched    -- the same engines advanced together in one batch;
@@ -594,16 +594,16 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
     fit_s = time.perf_counter() - t0
     held = systems[200:]
     t0 = time.perf_counter()
-    judged = plain_dos_many([(s, lo, hi, w, 10_000 + k) for k, (s, lo, hi, w) in enumerate(held)],
-                            final_factor=judge_factor, epoch_attempts=EPOCH_ATTEMPTS)
-    judge_s = time.perf_counter() - t0
-    judges = [np.where(d.valid, d.log_g, np.nan) for d in judged]
+    long_runs = plain_dos_many([(s, lo, hi, w, 10_000 + k) for k, (s, lo, hi, w) in enumerate(held)],
+                            final_factor=long_run_factor, epoch_attempts=EPOCH_ATTEMPTS)
+    long_run_s = time.perf_counter() - t0
+    references = [np.where(d.valid, d.log_g, np.nan) for d in long_runs]
     # the learned prior's own error, before any sampling
     prior_err = []
-    for (s, lo, hi, w), judge in zip(held, judges):
+    for (s, lo, hi, w), ref in zip(held, references):
         lg = model.predict_log_g(s, lo, hi, w)
-        prior_err.append(float(np.max(np.abs((lg - judge)[np.isfinite(judge)] -
-                                             np.nanmean(lg[np.isfinite(judge)] - judge[np.isfinite(judge)])))))
+        prior_err.append(float(np.max(np.abs((lg - ref)[np.isfinite(ref)] -
+                                             np.nanmean(lg[np.isfinite(ref)] - ref[np.isfinite(ref)])))))
 
     def engines(precision: str, learned: bool) -> list:
         out = []
@@ -626,7 +626,7 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
                                      ("combined", "fp32", True)):
         engs = engines(precision, learned)
         try:
-            r = batch_to_accuracy(engs, judges, tolerance, max_seconds=150.0)
+            r = batch_to_accuracy(engs, references, tolerance, max_seconds=150.0)
             r["ln_f_1e-8_s_extrapolated"] = to_ln_f_1e8(engs, r["attempts_per_walker_per_s"])
             if precision != "fp64":
                 reps = [e.precision_report() for e in engs]
@@ -649,7 +649,7 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
     for k in range(sequential_sample):
         s, lo, hi, w = held[k]
         with Engine(s, single_window_config(lo, hi, w, s.size(), 20_000 + k, 1e-8)) as e:
-            r = engine_to_accuracy(e, judges[k], tolerance, max_seconds=40.0)
+            r = engine_to_accuracy(e, references[k], tolerance, max_seconds=40.0)
             active = float(np.mean([x["active_bins"] for x in e.walker_statistics()]))
         r["ln_f_1e-8_s"] = active / 1e-8 / r["attempts_per_walker_per_s"]
         r["active_bins"] = active
@@ -701,9 +701,9 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
     seq_all = arms["plain_sequential"]["seconds_90pct_scaled"]
     out = {"tolerance": tolerance, "criterion": "max |d log g - mean| against the system's own long plain FP64 run",
            "systems": 256, "trained_on": 200, "held_out": len(held), "start_factor": start_factor,
-           "judge_final_factor": judge_factor,
+           "long_run_final_factor": long_run_factor,
            "training": {"curves": len(train), "final_loss": loss, "curve_seconds": curves_s, "fit_seconds": fit_s},
-           "setup_s": setup_s, "judge_s": judge_s,
+           "setup_s": setup_s, "long_run_s": long_run_s,
            "prior_error": {"median": float(np.median(prior_err)), "max": float(np.max(prior_err))},
            "arms": arms, "reference_cpu": cpu,
            "combined_over_plain_sequential": seq_all / comb if (seq_all and comb) else None,

@@ -6,7 +6,7 @@ is trained on DOS curves that the plain engine produces on generated systems; fo
 system it predicts log g over the run's grid, and the engine starts its walkers from that
 estimate at a small ln f (Engine.warm_start).  Plain Wang-Landau from a flat start stays the
 fallback: warm_start_or_flat returns the flat start whenever the prediction is unusable, and
-the plain method judges the error of the learned one.
+the plain method is the measure of the learned one's error.
 
 Prior: over uniformly random configurations the energy E = sum_{i<j} J_ij s_i s_j has mean 0,
 variance sigma^2 = sum_{i<j} J_ij^2 and third cumulant tr(J^3), so
@@ -331,10 +331,10 @@ def dilute_instance(k: int, seed0: int = 50_000):
     return s, -100.0 * w, 100.0 * w, w
 
 
-def accuracy_error(log_g: np.ndarray, valid: np.ndarray, judge_log_g: np.ndarray) -> float:
-    """max |d - mean(d)| with d = log g - judge over the bins the judge found (inf until all of
+def accuracy_error(log_g: np.ndarray, valid: np.ndarray, reference_log_g: np.ndarray) -> float:
+    """max |d - mean(d)| with d = log g - reference over the bins the reference found (inf until all of
     them are valid in the run)."""
-    ref = np.asarray(judge_log_g, dtype=np.float64)
+    ref = np.asarray(reference_log_g, dtype=np.float64)
     occ = np.isfinite(ref)
     if not np.all(np.asarray(valid)[occ] == 1):
         return math.inf
@@ -364,10 +364,10 @@ def single_window_config(emin: float, emax: float, width: float, n: int, seed: i
     return c
 
 
-def batch_to_accuracy(engines: Sequence[Engine], judges: Sequence[np.ndarray], tolerance: float,
+def batch_to_accuracy(engines: Sequence[Engine], references: Sequence[np.ndarray], tolerance: float,
                       chunk_epochs: int = 8, max_seconds: float = 600.0) -> dict:
     """Advances the engines together (one Batch: one CUDA-graph launch per step for all of them)
-    and, every chunk_epochs epochs, measures each engine's error against its judge.  Returns the
+    and, every chunk_epochs epochs, measures each engine's error against its reference run.  Returns the
     wall seconds and attempts per walker at which each engine first met the tolerance (None if
     not within max_seconds), the seconds until all had, and each engine's attempts per second
     over the run."""
@@ -382,11 +382,11 @@ def batch_to_accuracy(engines: Sequence[Engine], judges: Sequence[np.ndarray], t
         while True:
             batch.run_epochs(chunk_epochs)
             now = time.perf_counter() - t0
-            for k, (e, judge) in enumerate(zip(engines, judges)):
+            for k, (e, ref) in enumerate(zip(engines, references)):
                 if hit_s[k] is not None:
                     continue
                 frag = e.fragment(0, allow_empty=True)
-                errors[k] = accuracy_error(frag.log_g, frag.valid, judge)
+                errors[k] = accuracy_error(frag.log_g, frag.valid, ref)
                 if errors[k] <= tolerance:
                     hit_s[k] = now
                     hit_att[k] = e.totals()["attempted"] // e.walkers
@@ -400,7 +400,7 @@ def batch_to_accuracy(engines: Sequence[Engine], judges: Sequence[np.ndarray], t
             "attempts_per_walker_per_s": rates, "elapsed_s": elapsed}
 
 
-def engine_to_accuracy(engine: Engine, judge: np.ndarray, tolerance: float, chunk_epochs: int = 8,
+def engine_to_accuracy(engine: Engine, reference: np.ndarray, tolerance: float, chunk_epochs: int = 8,
                        max_seconds: float = 120.0) -> dict:
     """One engine alone, chunk_epochs epochs at a time, until its error meets the tolerance."""
     import time
@@ -409,7 +409,7 @@ def engine_to_accuracy(engine: Engine, judge: np.ndarray, tolerance: float, chun
     while True:
         engine.run_epochs(chunk_epochs)
         frag = engine.fragment(0, allow_empty=True)
-        err = accuracy_error(frag.log_g, frag.valid, judge)
+        err = accuracy_error(frag.log_g, frag.valid, reference)
         now = time.perf_counter() - t0
         if err <= tolerance or now > max_seconds:
             break

@@ -1,5 +1,5 @@
 """Mixed-precision runs: FP32 or BF16 (+ per-row FP32 scale) couplings with FP64 fields and a
-periodic FP64 recompute.  The plain FP64 engine and exact enumeration are the judges; the
+periodic FP64 recompute.  The plain FP64 engine and exact enumeration are the references; the
 reference has no low-precision path."""
 from __future__ import annotations
 
