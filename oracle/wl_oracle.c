@@ -684,7 +684,7 @@ int orc_walker_begin_next_iteration(orc_walker* w, char* err, size_t len) {
         if (w->time_offset == ORC_CONTINUE_SCHEDULE) {
             /* warm start continuing the schedule: 1/t from the factor reached, as if
              * round(active / factor) attempts had been made */
-            const double made = nearbyint((double)w->active_count / w->factor);
+            const double made = fmin(nearbyint((double)w->active_count / w->factor), 0x1.0p62);
             const double attempted = (double)w->attempted;
             w->time_offset = made > attempted ? (uint64_t)(made - attempted) : 0;
             w->stage = WLG_STAGE_INVERSE_TIME;

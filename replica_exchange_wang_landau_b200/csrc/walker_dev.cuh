@@ -110,7 +110,7 @@ __device__ __forceinline__ void warp_begin_next_iteration(WalkerState& st, uint6
         if (st.time_offset == kContinueSchedule) {
             // a warm start continuing the schedule: the 1/t stage starts at this check from the
             // factor reached, as if round(active / factor) attempts had been made
-            const double made = nearbyint(static_cast<double>(st.active_count) / st.factor);
+            const double made = fmin(nearbyint(static_cast<double>(st.active_count) / st.factor), 0x1.0p62);
             const double attempted = static_cast<double>(st.attempted);
             st.time_offset = made > attempted ? static_cast<uint64_t>(made - attempted) : 0;
             st.stage = kInverseTime;
