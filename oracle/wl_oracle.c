@@ -1000,20 +1000,28 @@ static int validate_config(const wlg_run_config* c, uint64_t bins_checked, char*
 
 /* The engine's FP32-couplings form (an extension; the reference stores J in FP64 only): walkers
  * are constructed from the FP64 couplings, then every accepted flip adds the FP32-rounded
- * coupling (update_value).  The engine's periodic FP64 recompute and resync have no restatement
- * here, so a run must end before the first one is due; BF16 is not restated. */
+ * coupling (update_value), and every R = ceil(recompute interval / exchange interval) epochs,
+ * after the epoch's exchange and unless the run has just terminated, every walker's fields and
+ * energy are recomputed from the FP64 couplings in the reference's order (local_fields,
+ * total_energy) and replace the drifted ones, unless the recomputed energy lies outside the
+ * walker's window (the resync is then deferred).  BF16 is not restated. */
 static int check_precision(const wlg_run_config* cfg, char* err, size_t len) {
-    if (cfg->coupling_precision == WLG_PRECISION_FP64) return 0;
-    if (cfg->coupling_precision != WLG_PRECISION_FP32) {
-        set_err(err, len, "the oracle restates FP64 and FP32 couplings only");
-        return 1;
+    if (cfg->coupling_precision == WLG_PRECISION_FP64 || cfg->coupling_precision == WLG_PRECISION_FP32) return 0;
+    set_err(err, len, "the oracle restates FP64 and FP32 couplings only");
+    return 1;
+}
+
+static void recompute_fp64(orc_walker* const* ws, uint64_t total, const orc_couplings* c) {
+    double* f64 = malloc(c->n * sizeof(double));
+    for (uint64_t q = 0; q < total; ++q) {
+        orc_walker* w = ws[q];
+        orc_local_fields(c, w->spins, f64);
+        const double e64 = orc_total_energy(c, w->spins);
+        if (!w_contains(w, w_index(w, e64))) continue; /* deferred */
+        memcpy(w->fields, f64, c->n * sizeof(double));
+        w->energy = e64;
     }
-    if (cfg->recompute_interval_attempts != 0 &&
-        (cfg->max_attempts == 0 || cfg->max_attempts >= cfg->recompute_interval_attempts)) {
-        set_err(err, len, "the oracle restates FP32 runs only up to their first FP64 recompute");
-        return 1;
-    }
-    return 0;
+    free(f64);
 }
 
 void orc_walker_warm_start(orc_walker* w, const double* log_g, double factor, int continue_schedule) {
@@ -1079,6 +1087,11 @@ orc_result* orc_run_rewl_warm(const orc_couplings* c, const wlg_run_config* cfg,
     uint64_t epoch = 0, last_checkpoint = 0;
     uint64_t* last_check = calloc(total, sizeof(uint64_t));
     const int unlimited = cfg->max_attempts == 0;
+    const uint64_t ex = cfg->exchange_interval_attempts;
+    const uint64_t recompute_epochs =
+        cfg->coupling_precision == WLG_PRECISION_FP32 && cfg->recompute_interval_attempts != 0
+            ? (cfg->recompute_interval_attempts + ex - 1) / ex
+            : 0;
     int done = 0, status = 0;
     while (!done && !status) {
         int limit_reached = !unlimited;
@@ -1119,6 +1132,10 @@ orc_result* orc_run_rewl_warm(const orc_couplings* c, const wlg_run_config* cfg,
             }
         }
         ++epoch;
+        int all_frozen_now = 1;
+        for (uint64_t q = 0; q < total; ++q) all_frozen_now &= ws[q]->stage == WLG_STAGE_FROZEN;
+        if (recompute_epochs && !(all_frozen_now || limit_reached) && epoch % recompute_epochs == 0)
+            recompute_fp64(ws, total, c);
         if (checkpointing && ws[0]->attempted - last_checkpoint >= cfg->checkpoint_interval_attempts) {
             save_checkpoint(cfg->checkpoint_path, ws[0]);
             last_checkpoint = ws[0]->attempted;

@@ -90,3 +90,18 @@ def test_csr_workload_bitwise(oracle, precision):
     assert got.exchange_attempted > 0
     assert results_equal(got, want) == []
 
+
+
+def test_mixed_precision_workload_fp32_bitwise(oracle):
+    """The mixed-precision configuration with FP32 couplings and the FP64 recompute after every
+    MCS (the bench's FP32 line): FP32-rounded couplings in every accepted flip, the recompute and
+    resync after every epoch, bit for bit against the oracle's restatement."""
+    system, configs = bench.mixed_precision_workload(precisions=("fp32",))
+    config = configs["fp32"]
+    config.max_mcs = 3.0
+    config.resolved_spin_count = 0
+    config.resolve_mcs(system.size())
+    got, _ = _run(system, config)
+    want = oracle.run_rewl(system, config)
+    assert got.precision_report["recomputes"] >= 2
+    assert results_equal(got, want) == []

@@ -8,7 +8,7 @@ import math
 import numpy as np
 import pytest
 
-from replica_exchange_wang_landau_b200.engine import Engine, RunConfig, System, WlParameters, run_rewl
+from replica_exchange_wang_landau_b200.engine import Engine, Geometry, RunConfig, System, WlParameters, run_rewl
 from replica_exchange_wang_landau_b200.geometry import simple_cubic_random
 
 pytestmark = pytest.mark.gpu
@@ -130,3 +130,23 @@ def test_split_sweep_matches_ring_sweep(precision):
     for a, b in zip(split, ring):
         assert snapshots_equal(a, b) == []
     assert rep_a["max_field_drift"] == rep_b["max_field_drift"]
+
+
+@pytest.mark.parametrize("recompute_mcs", [1.0, 6.0])
+def test_fp32_run_with_recompute_bitwise(oracle, recompute_mcs):
+    """FP32 couplings with the FP64 recompute every epoch (inside the epoch graph) and every
+    third epoch (between graph replays), on the split sweep, bit for bit against the oracle's
+    restatement of the recompute and resync."""
+    from helpers import random_axes, results_equal
+    g = Geometry.simple_cubic(5, 4, 4, periodic=True)
+    g.axes = random_axes(g.size(), 31)
+    s = System(g, 1.0, 0.0)
+    c = RunConfig(emin=-200, emax=200, bin_width=0.5, windows=3, walkers=2, seed=12, exchange_interval_mcs=2,
+                  check_interval_mcs=6, max_mcs=120)
+    c.coupling_precision = "fp32"
+    c.recompute_interval_mcs = recompute_mcs
+    c.resolve_mcs(s.size())
+    got = run_rewl(s, c)
+    want = oracle.run_rewl(s, c)
+    assert got.precision_report["recomputes"] >= (50 if recompute_mcs == 1.0 else 15)
+    assert results_equal(got, want) == []

@@ -193,38 +193,34 @@ def test_oracle_matches_compiled_reference(oracle, reference, seed):
 
 
 def test_oracle_refuses_what_it_does_not_restate(oracle):
-    """FP32 couplings are restated up to the first FP64 recompute only, and BF16 not at all."""
+    """BF16 couplings are not restated."""
     from oracle.oracle import CheckerError
     s = System(Geometry.simple_cubic(2, 2, 2, periodic=False))
     c = RunConfig(emin=-20, emax=20, bin_width=0.25, windows=1, walkers=1, seed=1, max_mcs=10)
-    c.coupling_precision = "fp32"
-    c.recompute_interval_mcs = 5.0
-    c.resolve_mcs(8)
-    with pytest.raises(CheckerError, match="first FP64 recompute"):
-        oracle.run_rewl(s, c)
     c.coupling_precision = "bf16"
+    c.resolve_mcs(8)
     with pytest.raises(CheckerError, match="FP64 and FP32"):
         oracle.run_rewl(s, c)
 
 
-def test_oracle_fp32_run_matches_fp32_walkers(oracle):
-    """An FP32 run_rewl of one walker equals the oracle walker with FP32 updates switched on
-    after construction (the engine's FP32 form: FP64 construction, FP32 coupling updates)."""
+def test_oracle_fp32_recompute_replaces_drifted_energies(oracle):
+    """The restated FP64 recompute of an FP32 run acts: with it every fourth MCS the walkers end
+    with other energies (exact FP64 totals) than the same FP32 run without it (drifted sums),
+    over the same attempts.  The GPU tests pin the restatement to the engine bit for bit."""
     g = Geometry.simple_cubic(3, 3, 2, periodic=True)
     g.axes = random_axes(18, 4)
     s = System(g, 1.0, 0.0)
-    c = RunConfig(emin=-40, emax=40, bin_width=0.5, windows=1, walkers=1, seed=6)
-    c.coupling_precision = "fp32"
-    c.recompute_interval_mcs = 0.0
-    c.max_mcs = 300
-    c.exchange_interval_mcs = 300
-    c.check_interval_mcs = 1000
-    c.resolve_mcs(18)
-    r = oracle.run_rewl(s, c)
-    w = oracle.walker(s, 0, c.emin, c.emax, c.bin_width, (0, c.bins()), c.wl, c.seed)
-    w.set_update_fp32(True)
-    w.run_attempts(c.max_attempts)
-    snap = w.snapshot()
-    assert r.attempted == c.max_attempts
-    assert float(r.walker_statistics[0]["energy"]).hex() == float(snap.energy).hex()
-    assert r.accepted == snap.accepted
+
+    def run(recompute_mcs):
+        c = RunConfig(emin=-40, emax=40, bin_width=0.5, windows=2, walkers=2, seed=6)
+        c.coupling_precision = "fp32"
+        c.exchange_interval_mcs = 2
+        c.recompute_interval_mcs = recompute_mcs
+        c.max_mcs = 40
+        c.check_interval_mcs = 10
+        c.resolve_mcs(18)
+        return oracle.run_rewl(s, c)
+
+    with_recompute, without = run(4.0), run(0.0)
+    assert with_recompute.attempted == without.attempted > 0
+    assert [x["energy"] for x in with_recompute.walker_statistics] != [x["energy"] for x in without.walker_statistics]
