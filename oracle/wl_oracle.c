@@ -108,6 +108,8 @@ struct orc_couplings {
     uint64_t* columns; /* CSR: nnz                                       */
     double* values;    /* CSR: nnz                                       */
     int update_fp32;   /* add_flip_delta with FP32-rounded couplings      */
+    int update_bf16;   /* add_flip_delta with BF16 couplings and row scale */
+    double* bf16_value; /* dense, n*n: row k holds scale_k * bf16(J_kj / scale_k) */
 };
 
 /* Geometry::validate (physics.cpp:34-56) */
@@ -209,7 +211,7 @@ orc_couplings* orc_couplings_create(const wlg_system* s, char* err, size_t len) 
 
 void orc_couplings_destroy(orc_couplings* c) {
     if (!c) return;
-    free(c->dense); free(c->offsets); free(c->columns); free(c->values);
+    free(c->dense); free(c->offsets); free(c->columns); free(c->values); free(c->bf16_value);
     free(c);
 }
 
@@ -258,7 +260,10 @@ static double update_value(const orc_couplings* c, double v) { return c->update_
 static void add_flip_delta(const orc_couplings* c, uint64_t flipped, int8_t old_spin, double* fields) {
     const double multiplier = -2.0 * (double)old_spin;
     const uint64_t n = c->n;
-    if (!c->csr) {
+    if (!c->csr && c->update_bf16) { /* the flipped site's BF16 row; every product is exact */
+        const double* row = c->bf16_value + flipped * n;
+        for (uint64_t j = 0; j < n; ++j) fields[j] += multiplier * row[j];
+    } else if (!c->csr) {
         for (uint64_t j = 0; j < n; ++j) fields[j] += multiplier * update_value(c, c->dense[j * n + flipped]);
     } else {
         for (uint64_t k = c->offsets[flipped]; k < c->offsets[flipped + 1]; ++k)
@@ -267,6 +272,34 @@ static void add_flip_delta(const orc_couplings* c, uint64_t flipped, int8_t old_
 }
 
 void orc_couplings_set_update_fp32(orc_couplings* c, int on) { c->update_fp32 = on != 0; }
+
+/* Round to nearest even at bfloat16's 8 significant bits (subnormal spacing 2^-133), directly
+ * from the double (one rounding, as the device's double-to-bf16 conversion does). */
+double orc_bf16_round(double x) {
+    if (x == 0.0 || !isfinite(x)) return x;
+    int e = 0;
+    (void)frexp(x, &e); /* |x| = m 2^e, 0.5 <= m < 1 */
+    int q = e - 8;
+    if (q < -133) q = -133;
+    return ldexp(nearbyint(ldexp(x, -q)), q);
+}
+
+/* The engine's BF16 form of dense couplings: per row k the scale s_k = (float) max_j |J_kj|
+ * (1 for a zero row) and the values bf16(J_kj / s_k); an accepted flip of site k adds
+ * (-2 s) * s_k * bf16(J_kj / s_k) to field j, a product exact in FP64. */
+void orc_couplings_set_update_bf16(orc_couplings* c, int on) {
+    c->update_bf16 = on != 0 && !c->csr;
+    if (!c->update_bf16 || c->bf16_value) return;
+    const uint64_t n = c->n;
+    c->bf16_value = malloc(n * n * sizeof(double));
+    for (uint64_t k = 0; k < n; ++k) {
+        double mx = 0.0;
+        for (uint64_t j = 0; j < n; ++j) mx = fmax(mx, fabs(c->dense[k * n + j]));
+        const float sc = mx > 0.0 ? (float)mx : 1.0f;
+        for (uint64_t j = 0; j < n; ++j)
+            c->bf16_value[k * n + j] = (double)sc * orc_bf16_round(c->dense[k * n + j] / (double)sc);
+    }
+}
 
 void orc_couplings_csr(const orc_couplings* c, uint64_t* offsets, uint64_t* columns, double* values) {
     if (!c->csr) return;
@@ -998,16 +1031,19 @@ static int validate_config(const wlg_run_config* c, uint64_t bins_checked, char*
     return 0;
 }
 
-/* The engine's FP32-couplings form (an extension; the reference stores J in FP64 only): walkers
- * are constructed from the FP64 couplings, then every accepted flip adds the FP32-rounded
- * coupling (update_value), and every R = ceil(recompute interval / exchange interval) epochs,
+/* The engine's FP32- and BF16-couplings forms (extensions; the reference stores J in FP64
+ * only): walkers are constructed from the FP64 couplings, then every accepted flip adds the
+ * FP32-rounded coupling (update_value) or the BF16 row value times its row scale
+ * (orc_couplings_set_update_bf16), and every R = ceil(recompute interval / exchange interval) epochs,
  * after the epoch's exchange and unless the run has just terminated, every walker's fields and
  * energy are recomputed from the FP64 couplings in the reference's order (local_fields,
  * total_energy) and replace the drifted ones, unless the recomputed energy lies outside the
- * walker's window (the resync is then deferred).  BF16 is not restated. */
+ * walker's window (the resync is then deferred). */
 static int check_precision(const wlg_run_config* cfg, char* err, size_t len) {
-    if (cfg->coupling_precision == WLG_PRECISION_FP64 || cfg->coupling_precision == WLG_PRECISION_FP32) return 0;
-    set_err(err, len, "the oracle restates FP64 and FP32 couplings only");
+    if (cfg->coupling_precision == WLG_PRECISION_FP64 || cfg->coupling_precision == WLG_PRECISION_FP32 ||
+        cfg->coupling_precision == WLG_PRECISION_BF16)
+        return 0;
+    set_err(err, len, "Unknown coupling precision");
     return 1;
 }
 
@@ -1039,6 +1075,10 @@ orc_result* orc_run_rewl_warm(const orc_couplings* c, const wlg_run_config* cfg,
                               double warm_factor, int continue_schedule, char* err, size_t len) {
     if (validate_config(cfg, 0, err, len)) return NULL;
     if (check_precision(cfg, err, len)) return NULL;
+    if (cfg->coupling_precision == WLG_PRECISION_BF16 && c->csr) {
+        set_err(err, len, "BF16 couplings are available for the dense backend only");
+        return NULL;
+    }
     uint64_t bins = 0;
     orc_grid_bins(cfg->emin, cfg->emax, cfg->bin_width, &bins);
     const uint64_t nw = cfg->windows, wpw = cfg->walkers_per_window, total = nw * wpw, n = c->n;
@@ -1070,8 +1110,9 @@ orc_result* orc_run_rewl_warm(const orc_couplings* c, const wlg_run_config* cfg,
     if (warm_log_g)
         for (uint64_t q = 0; q < total; ++q) orc_walker_warm_start(ws[q], warm_log_g, warm_factor, continue_schedule);
     /* FP32 couplings: the constructors above used FP64; the updates from here on use FP32 */
-    const int saved_update_fp32 = c->update_fp32;
+    const int saved_update_fp32 = c->update_fp32, saved_update_bf16 = c->update_bf16;
     if (cfg->coupling_precision == WLG_PRECISION_FP32) ((orc_couplings*)c)->update_fp32 = 1;
+    if (cfg->coupling_precision == WLG_PRECISION_BF16) orc_couplings_set_update_bf16((orc_couplings*)c, 1);
     const int checkpointing = cfg->checkpoint_path && cfg->checkpoint_path[0] && nw == 1 && wpw == 1;
     if (checkpointing) {
         int8_t* sp = malloc(n); double* fl = malloc(n * 8); double* lg = malloc(bins * 8);
@@ -1089,7 +1130,7 @@ orc_result* orc_run_rewl_warm(const orc_couplings* c, const wlg_run_config* cfg,
     const int unlimited = cfg->max_attempts == 0;
     const uint64_t ex = cfg->exchange_interval_attempts;
     const uint64_t recompute_epochs =
-        cfg->coupling_precision == WLG_PRECISION_FP32 && cfg->recompute_interval_attempts != 0
+        cfg->coupling_precision != WLG_PRECISION_FP64 && cfg->recompute_interval_attempts != 0
             ? (cfg->recompute_interval_attempts + ex - 1) / ex
             : 0;
     int done = 0, status = 0;
@@ -1146,6 +1187,7 @@ orc_result* orc_run_rewl_warm(const orc_couplings* c, const wlg_run_config* cfg,
     }
     free(last_check);
     ((orc_couplings*)c)->update_fp32 = saved_update_fp32;
+    ((orc_couplings*)c)->update_bf16 = saved_update_bf16;
     if (status) {
         for (uint64_t q = 0; q < total; ++q) orc_walker_destroy(ws[q]);
         free(ws); free(windows); orc_result_destroy(r);

@@ -32,6 +32,13 @@ uint64_t orc_couplings_nnz(const orc_couplings* c);
  * FP64.  Set it after a walker's construction to follow an FP32 engine walker, whose
  * initialisation uses the FP64 couplings. */
 void orc_couplings_set_update_fp32(orc_couplings* c, int on);
+/* Not in the reference: the update arithmetic of the engine's BF16 runs (dense couplings): per
+ * row k the scale s_k = (float) max_j |J_kj| and the values bf16(J_kj / s_k), rounded to nearest
+ * even directly from the double; an accepted flip of site k adds (-2 s) * s_k * bf16(J_kj / s_k). */
+void orc_couplings_set_update_bf16(orc_couplings* c, int on);
+/* bfloat16 rounding (8 significant bits, exponent range of float) of a double, to nearest even,
+ * in one step from the double; returned as the double it equals. */
+double orc_bf16_round(double x);
 /* The CSR arrays of a cutoff system: offsets[n+1], columns[nnz], values[nnz]. */
 void orc_couplings_csr(const orc_couplings* c, uint64_t* offsets, uint64_t* columns, double* values);
 void orc_couplings_dense(const orc_couplings* c, double* out);

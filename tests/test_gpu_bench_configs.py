@@ -7,9 +7,10 @@ run_rewl (src/parallel.cpp:276-534) on the identical system and configuration:
 * the dense REWL workload (8x8x8 periodic, random axes, 16 windows x 8 walkers, 913 bins of
   0.5, exchange every MCS): 1300 MCS, past the switch to the 1/t stage, through the split
   sweep (sweep_dense_split_kernel);
-* the mixed-precision configuration with FP64 couplings (16x16x16 lattice with 40% of the
-  sites removed, N = 2458, slab box (16, 16, 0), 32 windows x 8 walkers): 3 MCS through the
-  ring sweep for systems beyond 1024 sites;
+* the mixed-precision configuration with FP64, FP32 and row-scaled BF16 couplings (16x16x16
+  lattice with 40% of the sites removed, N = 2458, slab box (16, 16, 0), 32 windows x 8
+  walkers; FP64 recompute after every MCS for the FP32 and BF16 forms): 3 MCS through the ring
+  sweep for systems beyond 1024 sites;
 * the CSR configuration (32^3 periodic, cutoff 3.0, 122 neighbours in 128-wide ELLPACK rows,
   64 windows x 16 walkers = 1024 walkers, exchange every 0.05 MCS), FP64 and FP32 couplings:
   0.2 MCS through sweep_csr_kernel.  The bench seeds its windows from an adaptive pilot
@@ -92,12 +93,14 @@ def test_csr_workload_bitwise(oracle, precision):
 
 
 
-def test_mixed_precision_workload_fp32_bitwise(oracle):
-    """The mixed-precision configuration with FP32 couplings and the FP64 recompute after every
-    MCS (the bench's FP32 line): FP32-rounded couplings in every accepted flip, the recompute and
-    resync after every epoch, bit for bit against the oracle's restatement."""
-    system, configs = bench.mixed_precision_workload(precisions=("fp32",))
-    config = configs["fp32"]
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
+def test_mixed_precision_workload_low_precision_bitwise(oracle, precision):
+    """The mixed-precision configuration with FP32 (or row-scaled BF16) couplings and the FP64
+    recompute after every MCS (the bench's FP32 and BF16 lines): rounded couplings in every
+    accepted flip, the recompute and resync after every epoch, bit for bit against the oracle's
+    restatement."""
+    system, configs = bench.mixed_precision_workload(precisions=(precision,))
+    config = configs[precision]
     config.max_mcs = 3.0
     config.resolved_spin_count = 0
     config.resolve_mcs(system.size())

@@ -132,18 +132,20 @@ def test_split_sweep_matches_ring_sweep(precision):
     assert rep_a["max_field_drift"] == rep_b["max_field_drift"]
 
 
+@pytest.mark.parametrize("precision", ["fp32", "bf16"])
 @pytest.mark.parametrize("recompute_mcs", [1.0, 6.0])
-def test_fp32_run_with_recompute_bitwise(oracle, recompute_mcs):
-    """FP32 couplings with the FP64 recompute every epoch (inside the epoch graph) and every
-    third epoch (between graph replays), on the split sweep, bit for bit against the oracle's
-    restatement of the recompute and resync."""
+def test_low_precision_run_with_recompute_bitwise(oracle, precision, recompute_mcs):
+    """FP32 couplings, or BF16 couplings with their FP32 row scales, with the FP64 recompute
+    every epoch (inside the epoch graph) and every third epoch (between graph replays), on the
+    split sweep, bit for bit against the oracle's restatement of the update, the recompute and
+    the resync."""
     from helpers import random_axes, results_equal
     g = Geometry.simple_cubic(5, 4, 4, periodic=True)
     g.axes = random_axes(g.size(), 31)
     s = System(g, 1.0, 0.0)
     c = RunConfig(emin=-200, emax=200, bin_width=0.5, windows=3, walkers=2, seed=12, exchange_interval_mcs=2,
                   check_interval_mcs=6, max_mcs=120)
-    c.coupling_precision = "fp32"
+    c.coupling_precision = precision
     c.recompute_interval_mcs = recompute_mcs
     c.resolve_mcs(s.size())
     got = run_rewl(s, c)

@@ -192,15 +192,44 @@ def test_oracle_matches_compiled_reference(oracle, reference, seed):
         assert results_equal(oracle.run_rewl(s, c), reference.run_rewl(s, c)) == []
 
 
-def test_oracle_refuses_what_it_does_not_restate(oracle):
-    """BF16 couplings are not restated."""
+def test_oracle_refuses_what_the_engine_refuses(oracle):
+    """BF16 couplings exist for the dense backend only, in the restatement as in the engine."""
     from oracle.oracle import CheckerError
-    s = System(Geometry.simple_cubic(2, 2, 2, periodic=False))
+    s = System(Geometry.simple_cubic(3, 3, 3, periodic=True), 1.0, 1.8)
     c = RunConfig(emin=-20, emax=20, bin_width=0.25, windows=1, walkers=1, seed=1, max_mcs=10)
     c.coupling_precision = "bf16"
-    c.resolve_mcs(8)
-    with pytest.raises(CheckerError, match="FP64 and FP32"):
+    c.resolve_mcs(27)
+    with pytest.raises(CheckerError, match="dense backend only"):
         oracle.run_rewl(s, c)
+
+
+def _bf16_exact(x: float) -> float:
+    """Round-to-nearest-even to 8 significant bits (exponent floor 2^-133), in exact rationals."""
+    from fractions import Fraction
+    import math
+    if x == 0.0:
+        return x
+    q = max(math.frexp(x)[1] - 8, -133)
+    v = Fraction(x) / Fraction(2) ** q
+    n = math.floor(v)
+    r = v - n
+    if r > Fraction(1, 2) or (r == Fraction(1, 2) and n % 2 == 1):
+        n += 1
+    return math.ldexp(float(n), q)
+
+
+def test_bf16_rounding_is_round_to_nearest_even(oracle):
+    """The restated BF16 rounding: ties go to the even neighbour, a double just off a tie
+    rounds once (not through float first), and subnormal bfloat16 values keep 2^-133 steps."""
+    import ctypes as C
+    f = oracle.lib.orc_bf16_round
+    f.restype, f.argtypes = C.c_double, [C.c_double]
+    ties = [1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -8, -(1.0 + 2.0 ** -8), 1.0 + 2.0 ** -8 + 2.0 ** -40,
+            1.0 + 2.0 ** -8 - 2.0 ** -40, 2.0 ** -130 * 1.5, 2.0 ** -133 * 0.5, 2.0 ** -133 * 0.75]
+    assert [f(x) for x in ties[:5]] == [1.0, 1.0 + 2.0 ** -6, -1.0, 1.0 + 2.0 ** -7, 1.0]
+    rng = np.random.default_rng(8)
+    xs = ties + list(rng.normal(size=2000)) + list(rng.uniform(-1, 1, 2000) * 2.0 ** rng.integers(-140, 5, 2000))
+    assert [f(float(x)) for x in xs] == [_bf16_exact(float(x)) for x in xs]
 
 
 def test_oracle_fp32_recompute_replaces_drifted_energies(oracle):
