@@ -567,7 +567,30 @@ __device__ __forceinline__ double2 coupling_pair(const typename CouplingType<kPr
     }
 }
 
-template <int kChunks, bool kPow2, int kPrec, int kRL>
+// inverse_time_factor with a 32-bit count of active bins (a window has fewer than 2^31 bins)
+// and the no-active-bin case as a select, so that the table refresh is the only branch of the
+// per-attempt factor.
+struct InverseTimeTable32 {
+    double q = 0.0;         // lane j: active / (first + j + 1)
+    uint32_t active = 0;    // active-bin count of the block
+    uint32_t next = 32;     // the next attempt's lane; 32: no block
+};
+__device__ __forceinline__ double inverse_time_factor_select(InverseTimeTable32& T, uint64_t attempted_before,
+                                                             uint32_t active_bins, double current, int lane) {
+    if (T.next >= 32 || active_bins != T.active) {
+        T.active = active_bins;
+        T.next = 0;
+        T.q = static_cast<double>(active_bins) /
+              static_cast<double>(attempted_before + static_cast<uint64_t>(lane) + 1);
+    }
+    const double q = __shfl_sync(kFull, T.q, static_cast<int>(T.next++));
+    return active_bins == 0 ? current : q;
+}
+
+// kExact: ld == 64 * kChunks, every chunk of every lane is inside the row.  Otherwise the lower
+// half of the chunks still is (kChunks is the power of two at or above ceil(ld / 64)), and only
+// the upper half is masked.
+template <int kChunks, bool kPow2, int kPrec, int kRL, bool kExact>
 __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, WalkArgs a) {
     using JT = typename CouplingType<kPrec>::T;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -623,6 +646,8 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
     double2* fg2 = reinterpret_cast<double2*>(v.fields + static_cast<size_t>(st.slot) * ld);
     int8_t* sg = v.spins + static_cast<size_t>(st.slot) * ld;
     const int ld2 = ld >> 1;
+    // chunk k of this lane (column pair lane + 32 k) lies inside the row
+    auto inside = [&](int k, int c) { return kExact || k < kChunks / 2 || c < ld2; };
     double2 fr[kChunks];
     double2* f2s = reinterpret_cast<double2*>(f_s);
 
@@ -641,8 +666,8 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
 #pragma unroll
         for (int k = 0; k < kChunks; ++k) {
             const int c = lane + 32 * k;
-            fr[k] = c < ld2 ? fg2[c] : make_double2(0.0, 0.0);
-            if (c < ld2) f2s[c] = fr[k];
+            fr[k] = inside(k, c) ? fg2[c] : make_double2(0.0, 0.0);
+            if (inside(k, c)) f2s[c] = fr[k];
         }
         const int4* ssrc = reinterpret_cast<const int4*>(sg);
         int4* sdst = reinterpret_cast<int4*>(sp_s);
@@ -785,19 +810,41 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
     }
 
     // The attempts of one batch; kIT selects the 1/t stage (per-attempt factor and active
-    // count) or the Wang-Landau / frozen stages (constant factor).
-    auto run = [&](auto it_tag) {
+    // count) or the Wang-Landau / frozen stages (constant factor); kForce the forced acceptance
+    // (force_accept_after_attempts != 0), without which only the last acceptance is tracked.
+    auto run = [&](auto it_tag, auto force_tag) {
         constexpr bool kIT = decltype(it_tag)::value;
+        constexpr bool kForce = decltype(force_tag)::value;
+        uint32_t active32 = static_cast<uint32_t>(active_count);  // at most the window's bins
+        uint32_t acc_t = 0;  // without forced acceptance: the t of the last acceptance
         const bool frozen = stage == kFrozen;
-        InverseTimeTable itt;  // the 1/t factors of the coming attempts
+        InverseTimeTable32 itt;  // the 1/t factors of the coming attempts
         // 1/t stage: an attempt's factor and freeze are applied to log g of its bin at the point
         // where the next attempt first reads log g, so the factor's shuffle is not waited for
         double lg_base_p = 0.0, f_p = 0.0;
         bool pend = false;
         for (uint32_t t = 0; t < batch;) {
-            if (static_cast<int32_t>(hq + 4 - ready_to) >= 0 && !ensure(hq + 4)) {
-                failed = true;
-                break;
+            // the two rare cases share one branch: draws still in flight, and a site draw that
+            // bounded() rejected
+            const bool wait_draws = static_cast<int32_t>(hq + 4 - ready_to) >= 0;
+            if (wait_draws || i < 0) {
+                if (wait_draws && !ensure(hq + 4)) {
+                    failed = true;
+                    break;
+                }
+                if (i < 0) {  // bounded() rejects draw hq; the next draw is the candidate site
+                    const JT* prow = ring + static_cast<size_t>(prev_slot) * row_stride;
+                    hq += 1;
+                    i = c1;
+                    if (i >= 0) {
+                        si = sp_s[i];
+                        h = fma(m_prev, coupling<kPrec>(prow, i), f_s[i]);
+                    }
+                    c1 = c2;
+                    c2 = rec_site[(hq + 2) & qm];
+                    lnu = rec_lnu[(hq + 1) & qm];
+                    continue;
+                }
             }
             // Look ahead at the next batch without blocking; the result is used at the end
             // of the attempt, so the test's latency overlaps the chain.  Every batch before
@@ -805,18 +852,6 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
             const uint32_t next_batch = ready_to >> 2;
             const bool next_ready = mbar_test(bar_addr + 8 * (next_batch & bm), (next_batch >> blog) & 1u);
             const JT* prow = ring + static_cast<size_t>(prev_slot) * row_stride;
-            if (i < 0) {  // rare: bounded() rejects draw hq; the next draw is the candidate site
-                hq += 1;
-                i = c1;
-                if (i >= 0) {
-                    si = sp_s[i];
-                    h = fma(m_prev, coupling<kPrec>(prow, i), f_s[i]);
-                }
-                c1 = c2;
-                c2 = rec_site[(hq + 2) & qm];
-                lnu = rec_lnu[(hq + 1) & qm];
-                continue;
-            }
             const uint32_t slot = hq & qm;
             const JT* row = ring + static_cast<size_t>(slot) * row_stride;
             // loads: the next attempt's records, the candidates' fields, spins and couplings,
@@ -847,7 +882,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
 #pragma unroll
             for (int k = 0; k < kChunks; ++k) {
                 const int cc = lane + 32 * k;
-                rb[k] = cc < ld2 ? coupling_pair<kPrec>(prow, cc) : make_double2(0.0, 0.0);
+                rb[k] = inside(k, cc) ? coupling_pair<kPrec>(prow, cc) : make_double2(0.0, 0.0);
             }
             // the previous attempt's add_flip_delta (m_prev = 0 leaves every field unchanged)
 #pragma unroll
@@ -865,7 +900,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
             const double lg_new = nb == cur ? lg_cur : lg_load;
             const double log_ratio = lg_cur - lg_new;
             const bool det = log_ratio >= 0.0;
-            const bool forced = !det && since >= force_limit;
+            const bool forced = kForce && !det && since >= force_limit;
             const bool need_u = in_window && !det && !forced;
             const bool accepted = in_window && (det || forced || lnu < log_ratio);
 
@@ -876,22 +911,25 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
             const double h_next = fma(m_eff, need_u ? r2 : r1, need_u ? fc2 : fc1);
             const int s_next = (accepted && c == i) ? -si : (need_u ? s2 : s1);
             E = accepted ? Ep : E;
-            since = accepted ? 0 : since + 1;
             n_acc += accepted ? 1u : 0u;
-            n_forced += (accepted && forced) ? 1u : 0u;
+            if constexpr (kForce) {
+                since = accepted ? 0 : since + 1;
+                n_forced += (accepted && forced) ? 1u : 0u;
+            }
             ++t;
+            if constexpr (!kForce) acc_t = accepted ? t : acc_t;
 
             // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
-            if (kIT && stage == kInverseTime) {  // resolved at the next read of log g
-                f_p = inverse_time_factor(itt, att0 + st.time_offset + t - 1, active_count, factor, lane);
-                pend = true;
+            if (kIT) {  // resolved at the next read of log g; nothing pends once frozen
+                f_p = inverse_time_factor_select(itt, att0 + st.time_offset + t - 1, active32, factor, lane);
+                pend = stage == kInverseTime;
             }
             const bool move = accepted && nb != cur;
             const int ncur = move ? nb : cur;
             const double lg_base = move ? lg_new : lg_cur;
             if (kIT) {
                 const bool visited = act_s[ncur - wb] != 0;
-                active_count += visited ? 0 : 1;
+                active32 += visited ? 0u : 1u;
             }
 
             // stores: the fields up to the previous attempt, the flipped spin, log g of the
@@ -899,9 +937,16 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
 #pragma unroll
             for (int k = 0; k < kChunks; ++k) {
                 const int cc = lane + 32 * k;
-                if (cc < ld2) f2s[cc] = fr[k];
+                if (inside(k, cc)) f2s[cc] = fr[k];
             }
-            if (lane == 0) {
+            // Wang-Landau stage: every lane stores the same values (no branch), lane 0 counts
+            // the visit; the 1/t stage keeps them in lane 0's branch (measured faster there)
+            if constexpr (!kIT) {
+                sp_s[i] = static_cast<int8_t>(accepted ? -si : si);
+                lg_s[cur - wb] = lg_cur;
+                act_s[ncur - wb] = 1;
+                if (lane == 0) atomicAdd(&hd[ncur - wb], 1u);
+            } else if (lane == 0) {
                 if (accepted) sp_s[i] = static_cast<int8_t>(-si);
                 lg_s[cur - wb] = lg_cur;
                 atomicAdd(&hd[ncur - wb], 1u);
@@ -916,7 +961,8 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
             }
 
             __syncwarp();  // the stores are visible to every lane
-            if (lane == 0) st_release_shared(consumed_addr, hq);  // draws before this site are done
+            // draws before this site are done (in the Wang-Landau stage every lane stores the value)
+            if (!kIT || lane == 0) st_release_shared(consumed_addr, hq);
             hq += need_u ? 2u : 1u;
             i = c;
             si = s_next;
@@ -928,6 +974,8 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
             prev_slot = slot;
             ready_to += __all_sync(kFull, next_ready) ? static_cast<uint32_t>(kDrawBatch) : 0u;
         }
+        if constexpr (!kForce) since = n_acc ? static_cast<uint64_t>(batch - acc_t) : since + batch;
+        if (kIT) active_count = active32;
         if (kIT && pend) {  // the last attempt's factor
             const bool frz = f_p <= P.final_factor;
             stage = frz ? kFrozen : stage;
@@ -936,17 +984,20 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
         }
     };
     if (!failed) {
-        if (stage == kInverseTime)
-            run(std::true_type{});
-        else
-            run(std::false_type{});
+        if (P.force_after != 0) {
+            if (stage == kInverseTime) run(std::true_type{}, std::true_type{});
+            else run(std::false_type{}, std::true_type{});
+        } else {
+            if (stage == kInverseTime) run(std::true_type{}, std::false_type{});
+            else run(std::false_type{}, std::false_type{});
+        }
     }
     if (!failed) {  // the last attempt's field update
         const JT* prow = ring + static_cast<size_t>(prev_slot) * row_stride;
 #pragma unroll
         for (int k = 0; k < kChunks; ++k) {
             const int cc = lane + 32 * k;
-            if (cc < ld2) {
+            if (inside(k, cc)) {
                 const double2 r = coupling_pair<kPrec>(prow, cc);
                 fr[k].x = fma(m_prev, r.x, fr[k].x);
                 fr[k].y = fma(m_prev, r.y, fr[k].y);
@@ -1002,7 +1053,7 @@ __global__ void __launch_bounds__(64, 1) sweep_dense_split_kernel(EngineView v, 
 #pragma unroll
     for (int k = 0; k < kChunks; ++k) {
         const int c = lane + 32 * k;
-        if (c < ld2) fg2[c] = fr[k];
+        if (inside(k, c)) fg2[c] = fr[k];
     }
     {
         const int4* ssrc = reinterpret_cast<const int4*>(sp_s);
@@ -1039,16 +1090,21 @@ SweepFn sweep_fn() {
 
 }  // namespace
 
-template <int K, bool kPow2, int kPrec, int kRL>
-SweepFn split_fn() {
+template <int K, bool kPow2, int kPrec, int kRL, bool kExact>
+SweepFn split_fn_exact() {
     static bool configured = false;
     if (!configured) {
-        check_cuda(cudaFuncSetAttribute(reinterpret_cast<const void*>(&sweep_dense_split_kernel<K, kPow2, kPrec, kRL>),
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+        check_cuda(cudaFuncSetAttribute(
+                       reinterpret_cast<const void*>(&sweep_dense_split_kernel<K, kPow2, kPrec, kRL, kExact>),
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
                    "cudaFuncSetAttribute");
         configured = true;
     }
-    return &sweep_dense_split_kernel<K, kPow2, kPrec, kRL>;
+    return &sweep_dense_split_kernel<K, kPow2, kPrec, kRL, kExact>;
+}
+template <int K, bool kPow2, int kPrec, int kRL>
+SweepFn split_fn(int ld) {
+    return ld == 64 * K ? split_fn_exact<K, kPow2, kPrec, kRL, true>() : split_fn_exact<K, kPow2, kPrec, kRL, false>();
 }
 
 // Chunks of 64 couplings per lane pass, rounded up to a power of two (unused chunks are
@@ -1056,11 +1112,11 @@ SweepFn split_fn() {
 template <bool kPow2, int kPrec, int kRL>
 SweepFn pick_split_chunks(int ld) {
     const int chunks = (ld + 63) / 64;
-    if (chunks <= 1) return split_fn<1, kPow2, kPrec, kRL>();
-    if (chunks <= 2) return split_fn<2, kPow2, kPrec, kRL>();
-    if (chunks <= 4) return split_fn<4, kPow2, kPrec, kRL>();
-    if (chunks <= 8) return split_fn<8, kPow2, kPrec, kRL>();
-    if (chunks <= 16) return split_fn<16, kPow2, kPrec, kRL>();
+    if (chunks <= 1) return split_fn<1, kPow2, kPrec, kRL>(ld);
+    if (chunks <= 2) return split_fn<2, kPow2, kPrec, kRL>(ld);
+    if (chunks <= 4) return split_fn<4, kPow2, kPrec, kRL>(ld);
+    if (chunks <= 8) return split_fn<8, kPow2, kPrec, kRL>(ld);
+    if (chunks <= 16) return split_fn<16, kPow2, kPrec, kRL>(ld);
     return nullptr;
 }
 
