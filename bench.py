@@ -572,6 +572,10 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
                           the 1/t schedule;
       combined         -- batched, FP32 couplings with an FP64 recompute every epoch, learned
                           warm start (the batched + mixed-precision + learned form).
+    Times are run seconds: the wall time of the run calls, which return when their epochs are
+    done; the accuracy checks between them (every 8 epochs, a copy of each system's log g and a
+    comparison with its reference on the host) are the measurement's, not the method's, and are
+    left out of every arm alike (each arm's wall time with them is reported beside).
     Time to ln f <= 1e-8 of each arm is extrapolated from its measured attempts per walker per
     second (1/t: active bins / 1e-8 attempts per walker, less the continued schedule's offset).
     The reference's run_rewl (compiled from its sources, 2 walkers on 2 host threads) is timed
@@ -644,6 +648,7 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
                       if hits else None,
                       "max_final_error": max(r["final_errors"]),
                       "ln_f_1e-8_s_extrapolated": r["ln_f_1e-8_s_extrapolated"],
+                      "wall_s_with_checks": r["wall_s"],
                       **({k: r[k] for k in ("max_field_drift", "bin_changes") if k in r})}
     seq = []
     for k in range(sequential_sample):
@@ -658,6 +663,7 @@ def learned_configuration_line(tolerance: float = 0.02, start_factor: float = 1e
     per_system = float(np.mean([r["seconds"] for r in ok])) if ok else None
     arms["plain_sequential"] = {
         "systems_timed": len(seq), "reached": len(ok), "mean_seconds_per_system": per_system,
+        "mean_wall_s_with_checks_per_system": float(np.mean([r["wall_s"] for r in seq])),
         "seconds_all_56_scaled": per_system * len(held) if per_system else None,
         "seconds_90pct_scaled": per_system * np.ceil(0.9 * len(held)) if per_system else None,
         "median_attempts_per_walker": float(np.median([r["attempts_per_walker"] for r in ok])) if ok else None,
