@@ -247,28 +247,38 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
             }
 
             // The attempts of one batch; kIT selects the 1/t stage (per-attempt factor and
-            // active count) or the Wang-Landau / frozen stages (constant factor).
-            auto run = [&](auto it_tag) {
+            // active count) or the Wang-Landau / frozen stages (constant factor); kForce the
+            // forced acceptance (force_accept_after_attempts != 0), without which only the last
+            // acceptance is tracked.
+            auto run = [&](auto it_tag, auto force_tag) {
                 constexpr bool kIT = decltype(it_tag)::value;
+                constexpr bool kForce = decltype(force_tag)::value;
+                uint32_t acc_t = 0;  // without forced acceptance: the t of the last acceptance
+                uint32_t active32 = static_cast<uint32_t>(active_count);  // at most the window's bins
                 const bool frozen = stage == kFrozen;
-                InverseTimeTable itt;  // the 1/t factors of the coming attempts
+                InverseTimeTable32 itt;  // the 1/t factors of the coming attempts
                 // 1/t stage: an attempt's factor and freeze are applied to log g of its bin at the point
                 // where the next attempt first reads log g, so the factor's shuffle is not waited for
                 double lg_base_p = 0.0, f_p = 0.0;
                 bool pend = false;
                 for (uint32_t t = 0; t < batch;) {
-                    if (static_cast<int32_t>(hq + 4 - avail) >= 0 && !ensure(hq + 4)) {
-                        failed = true;
-                        break;
-                    }
-                    if (i < 0) {  // rare: bounded() rejects draw hq; the next draw is the site
-                        hq += 1;
-                        i = c1;
-                        h = __shfl_sync(kFull, f, i < 0 ? 0 : i);
-                        c1 = c2;
-                        c2 = rec_site[(hq + 2) & kWindowRingMask];
-                        lnu = rec_lnu[(hq + 1) & kWindowRingMask];
-                        continue;
+                    // the two rare cases share one branch: draws not yet in the ring, and a site
+                    // draw that bounded() rejected
+                    const bool wait_draws = static_cast<int32_t>(hq + 4 - avail) >= 0;
+                    if (wait_draws || i < 0) {
+                        if (wait_draws && !ensure(hq + 4)) {
+                            failed = true;
+                            break;
+                        }
+                        if (i < 0) {  // bounded() rejects draw hq; the next draw is the site
+                            hq += 1;
+                            i = c1;
+                            h = __shfl_sync(kFull, f, i < 0 ? 0 : i);
+                            c1 = c2;
+                            c2 = rec_site[(hq + 2) & kWindowRingMask];
+                            lnu = rec_lnu[(hq + 1) & kWindowRingMask];
+                            continue;
+                        }
                     }
                     // loads: the couplings of the site, the candidates' fields, the next records
                     const int c1l = c1 < 0 ? 0 : c1, c2l = c2 < 0 ? 0 : c2;
@@ -298,7 +308,7 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                     const double lg_new = nb == cur ? lg_cur : lg_load;
                     const double log_ratio = lg_cur - lg_new;
                     const bool det = log_ratio >= 0.0;
-                    const bool forced = !det && since >= force_limit;
+                    const bool forced = kForce && !det && since >= force_limit;
                     const bool need_u = in_window && !det && !forced;
                     const bool accepted = in_window && (det || forced || lnu < log_ratio);
 
@@ -309,24 +319,33 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                     const double h_next = fma(m_eff, need_u ? r2 : r1, need_u ? fc2 : fc1);
                     down ^= accepted ? (1u << i) : 0u;
                     E = accepted ? Ep : E;
-                    since = accepted ? 0 : since + 1;
                     n_acc += accepted ? 1u : 0u;
-                    n_forced += (accepted && forced) ? 1u : 0u;
+                    if constexpr (kForce) {
+                        since = accepted ? 0 : since + 1;
+                        n_forced += (accepted && forced) ? 1u : 0u;
+                    }
                     ++t;
+                    if constexpr (!kForce) acc_t = accepted ? t : acc_t;
 
                     // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
-                    if (kIT && stage == kInverseTime) {  // resolved at the next read of log g
-                        f_p = inverse_time_factor(itt, att0 + st.time_offset + t - 1, active_count, factor, lane);
-                        pend = true;
+                    if (kIT) {  // resolved at the next read of log g; nothing pends once frozen
+                        f_p = inverse_time_factor_select(itt, att0 + st.time_offset + t - 1, active32, factor, lane);
+                        pend = stage == kInverseTime;
                     }
                     const bool move = accepted && nb != cur;
                     const int ncur = move ? nb : cur;
                     const double lg_base = move ? lg_new : lg_cur;
                     if (kIT) {
                         const bool visited = act_s[ncur - wb] != 0;
-                        active_count += visited ? 0 : 1;
+                        active32 += visited ? 0u : 1u;
                     }
-                    if (lane == 0) {
+                    // Wang-Landau stage: every lane stores the same values (no branch), lane 0
+                    // counts the visit; the 1/t stage keeps them in lane 0's branch
+                    if constexpr (!kIT) {
+                        lg_s[cur - wb] = lg_cur;
+                        act_s[ncur - wb] = 1;
+                        if (lane == 0) atomicAdd(&hd[ncur - wb], 1u);
+                    } else if (lane == 0) {
                         lg_s[cur - wb] = lg_cur;
                         atomicAdd(&hd[ncur - wb], 1u);
                         act_s[ncur - wb] = 1;
@@ -339,7 +358,8 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                         lg_cur = frozen ? lg_base : lg_base + factor;
                     }
                     __syncwarp();  // the stores are visible to every lane
-                    if (lane == 0) st_release_u32(consumed_addr, hq);  // draws before this site are done
+                    // draws before this site are done (in the Wang-Landau stage every lane stores the value)
+                    if (!kIT || lane == 0) st_release_u32(consumed_addr, hq);
                     hq += need_u ? 2u : 1u;
                     i = c;
                     h = h_next;
@@ -347,6 +367,8 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                     c2 = need_u ? r4 : r3;
                     lnu = need_u ? l3 : l2;
                 }
+                if constexpr (!kForce) since = n_acc ? static_cast<uint64_t>(batch - acc_t) : since + batch;
+                if (kIT) active_count = active32;
                 if (kIT && pend) {  // the last attempt's factor
                     const bool frz = f_p <= P.final_factor;
                     stage = frz ? kFrozen : stage;
@@ -354,10 +376,13 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                     lg_cur = frz ? lg_base_p : lg_base_p + f_p;
                 }
             };
-            if (stage == kInverseTime)
-                run(std::true_type{});
-            else
-                run(std::false_type{});
+            if (P.force_after != 0) {
+                if (stage == kInverseTime) run(std::true_type{}, std::true_type{});
+                else run(std::false_type{}, std::true_type{});
+            } else {
+                if (stage == kInverseTime) run(std::true_type{}, std::false_type{});
+                else run(std::false_type{}, std::false_type{});
+            }
 
             if (failed) {
                 if (lane == 0) record_error(ctl, WLG_ERR_TIMEOUT, w);

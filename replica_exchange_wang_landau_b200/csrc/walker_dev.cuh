@@ -154,6 +154,26 @@ __device__ __forceinline__ double inverse_time_factor(InverseTimeTable& T, uint6
     return __shfl_sync(kFull, T.q, static_cast<int>(T.next++));
 }
 
+// inverse_time_factor with a 32-bit count of active bins (a window has fewer than 2^31 bins)
+// and the no-active-bin case as a select, so that the table refresh is the only branch of the
+// per-attempt factor.
+struct InverseTimeTable32 {
+    double q = 0.0;         // lane j: active / (first + j + 1)
+    uint32_t active = 0;    // active-bin count of the block
+    uint32_t next = 32;     // the next attempt's lane; 32: no block
+};
+__device__ __forceinline__ double inverse_time_factor_select(InverseTimeTable32& T, uint64_t attempted_before,
+                                                             uint32_t active_bins, double current, int lane) {
+    if (T.next >= 32 || active_bins != T.active) {
+        T.active = active_bins;
+        T.next = 0;
+        T.q = static_cast<double>(active_bins) /
+              static_cast<double>(attempted_before + static_cast<uint64_t>(lane) + 1);
+    }
+    const double q = __shfl_sync(kFull, T.q, static_cast<int>(T.next++));
+    return active_bins == 0 ? current : q;
+}
+
 // Floor of a bin coordinate 0 <= q < 2^31 (the grid index of an in-range energy): the sum
 // q + 2^52 rounded toward -infinity is 2^52 + floor(q) exactly (the unit in the last place is
 // 1 there), and its low word is floor(q).  One add instead of a double-to-integer conversion.
