@@ -141,6 +141,13 @@ def reduce_over_ranks(dist, device, maxima, sums):
     return t.tolist(), c.tolist()
 
 
+def apply_launch(eng, launch: dict) -> None:
+    """Gives an engine the launch shape an autotune report chose."""
+    eng.set_launch(launch["walkers_per_block"], launch["epochs_per_graph"])
+    if launch["staging_ring"]:
+        eng.set_staging_ring(launch["staging_ring"])
+
+
 def run_ours(args, rank: int, world: int, dist, torch) -> None:
     from replica_exchange_wang_landau_b200 import engine as E
     from replica_exchange_wang_landau_b200._abi import wlg_run_config
@@ -150,7 +157,13 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
     system, config = make_workload(seed=1 + rank)
     n = system.size()
     flush = torch.zeros(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    # the launch shape (staging ring, epochs per graph replay) from the engine's autotuner, run on
+    # a separate engine of the same system and configuration, so that the timed engine's epochs
+    # are the epochs it would run without the tuning
+    with E.Engine(system, config) as tuner:
+        launch = tuner.autotune(16)
     eng = E.Engine(system, config)
+    apply_launch(eng, launch)
     epochs = args.epochs_per_step
     for _ in range(args.warmup):
         eng.time_run(epochs)
@@ -175,6 +188,7 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
     # steps' epochs, launched one kernel at a time with CUDA events around every launch.  The
     # trajectories are deterministic, so these are the same attempts (checked below).
     twin = E.Engine(system, config)
+    apply_launch(twin, launch)
     for _ in range(args.warmup):
         twin.time_epochs(epochs)
     walk_ms = exch_ms = 0.0
@@ -237,6 +251,10 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
         cfg_s, keep = config._struct(n)
         handle = C.c_void_p()
         E._check(lib.wlg_engine_create(C.byref(sys_s), C.byref(cfg_s), C.byref(handle)))
+        # the tuned staging ring; the graph length stays the default 32 epochs, whose capture costs a
+        # fresh engine less than the tuned 64-epoch graphs of the long-running engine
+        if launch["staging_ring"]:
+            E._check(lib.wlg_engine_set_staging_ring(handle, launch["staging_ring"]))
         ran, done = C.c_uint64(0), C.c_int32(0)
         E._check(lib.wlg_engine_run_epochs(handle, epochs, C.byref(ran), C.byref(done)))
         E._check(lib.wlg_engine_fragments(handle, 0, p_lg, p_h, p_se, p_v))  # every window's fragment
@@ -273,16 +291,21 @@ def run_ours(args, rank: int, world: int, dist, torch) -> None:
             "config": {"workload": WORKLOAD, "walkers": 128, "spins": n, "epochs_per_step": epochs,
                        "attempts_per_step_per_gpu": attempted // args.steps,
                        "l2": "flushed between timed steps (256 MiB write); J (2 MB) is L2-resident within a step",
+                       "launch": {k: launch[k] for k in ("walkers_per_block", "epochs_per_graph", "staging_ring")},
+                       "launch_chosen_by": "wlg_engine_autotune (16 trial epochs per candidate, two passes) on a "
+                                           "separate engine of the same system and configuration",
                        "parallelism": f"{world} independent replica(s), one per GPU"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "steps": e2e_steps, "path": "wlg_engine_create -> wlg_engine_run_epochs -> wlg_engine_fragments "
+                    "steps": e2e_steps, "path": "wlg_engine_create -> wlg_engine_set_staging_ring (the tuned ring) "
+                                                "-> wlg_engine_run_epochs -> wlg_engine_fragments "
                                                 "(all 16 windows) -> wlg_engine_destroy, pinned host buffers",
                     "acceptance": e2e_accepted / max(1, e2e_attempts),
                     "note": "each step is a fresh engine's first epochs; acceptance, and with it the cost of an "
                             "attempt, differs from the long-running engine of value"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                         "kernel": "sweep_dense_split_kernel<8, pow2 width> (FP64 dense J)", "peak_source": peaks["source"],
+                         "kernel": f"sweep_dense_split_kernel<8, pow2 width> (FP64 dense J, "
+                                   f"{launch['staging_ring']}-draw staging ring)", "peak_source": peaks["source"],
                          "bytes_per_launch": bytes_per_launch, "launch_ms": launch_s * 1e3,
                          "acceptance": kt["accepted"] / max(1, kt["attempted"]),
                          "kernel_timing": f"the {k_launches} timed epochs (warm-up excluded), replayed after the "
