@@ -204,6 +204,11 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
         }
         return false;
     };
+    // The producer needs to know only when a whole batch of 32 draws has been consumed (its
+    // room test is per batch), so the consumed count is published when the draw index has
+    // entered a new batch (hq and the last published count differ above bit 4), from the rare
+    // branch at the top of an attempt, not after every attempt.
+    uint32_t published = 0;
     int i = 0, c1 = 0, c2 = 0;  // current site; candidates for the next one
     double h = 0.0, lnu = 0.0;  // field of the current site; log uniform of draw hq+1
     if (!failed) {
@@ -255,6 +260,11 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                 constexpr bool kForce = decltype(force_tag)::value;
                 uint32_t acc_t = 0;  // without forced acceptance: the t of the last acceptance
                 uint32_t active32 = static_cast<uint32_t>(active_count);  // at most the window's bins
+                // the current bin's histogram delta and visited flag, kept in registers like its
+                // log g (lg_cur); the shared copies are written every attempt and read only for
+                // the proposed bin, together with its log g
+                uint32_t hcnt = hd[cur - wb];
+                bool cur_vis = act_s[cur - wb] != 0;
                 const bool frozen = stage == kFrozen;
                 InverseTimeTable32 itt;  // the 1/t factors of the coming attempts
                 // 1/t stage: an attempt's factor and freeze are applied to log g of its bin at the point
@@ -262,10 +272,19 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                 double lg_base_p = 0.0, f_p = 0.0;
                 bool pend = false;
                 for (uint32_t t = 0; t < batch;) {
-                    // the two rare cases share one branch: draws not yet in the ring, and a site
-                    // draw that bounded() rejected
+                    // the rare cases share one branch: a consumed count to publish, draws not yet
+                    // in the ring, a site draw that bounded() rejected, and (1/t stage) a refresh
+                    // of the factor table (every 32 attempts, or when the active count changed)
+                    const bool publish = (hq ^ published) >= 32u;
                     const bool wait_draws = static_cast<int32_t>(hq + 4 - avail) >= 0;
-                    if (wait_draws || i < 0) {
+                    bool rare = publish || wait_draws || i < 0;
+                    if constexpr (kIT) rare = rare || itt.next >= 32 || active32 != itt.active;
+                    if (rare) {
+                        if (publish) {
+                            __syncwarp();  // every lane's reads of the consumed records come first
+                            if (lane == 0) st_release_u32(consumed_addr, hq);
+                            published = hq;
+                        }
                         if (wait_draws && !ensure(hq + 4)) {
                             failed = true;
                             break;
@@ -278,6 +297,10 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                             c2 = rec_site[(hq + 2) & kWindowRingMask];
                             lnu = rec_lnu[(hq + 1) & kWindowRingMask];
                             continue;
+                        }
+                        if constexpr (kIT) {
+                            if (itt.next >= 32 || active32 != itt.active)
+                                inverse_time_refresh(itt, att0 + st.time_offset + t, active32, lane);
                         }
                     }
                     // loads: the couplings of the site, the candidates' fields, the next records
@@ -297,7 +320,10 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                     int nb = in_range ? bin_floor(qv) : -1;
                     nb = (nb == gcount && Ep == g.maximum) ? gcount - 1 : nb;
                     const bool in_window = nb >= wb && nb < we;
-                    const double lg_load = lg_s[in_window ? nb - wb : 0];
+                    const int nl = in_window ? nb - wb : 0;
+                    const double lg_load = lg_s[nl];
+                    const uint32_t hd_load = hd[nl];
+                    const bool act_load = act_s[nl] != 0;
                     if (kIT) {  // the previous attempt's factor (update_inverse_time_factor) and log g update
                         const bool frz = pend && f_p <= P.final_factor;
                         stage = frz ? kFrozen : stage;
@@ -329,27 +355,23 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
 
                     // update_inverse_time_factor then update_current_bin (src/wang_landau.cpp:277-278)
                     if (kIT) {  // resolved at the next read of log g; nothing pends once frozen
-                        f_p = inverse_time_factor_select(itt, att0 + st.time_offset + t - 1, active32, factor, lane);
+                        f_p = inverse_time_factor_next(itt, active32, factor);
                         pend = stage == kInverseTime;
                     }
                     const bool move = accepted && nb != cur;
                     const int ncur = move ? nb : cur;
                     const double lg_base = move ? lg_new : lg_cur;
                     if (kIT) {
-                        const bool visited = act_s[ncur - wb] != 0;
+                        const bool visited = move ? act_load : cur_vis;
                         active32 += visited ? 0u : 1u;
                     }
-                    // Wang-Landau stage: every lane stores the same values (no branch), lane 0
-                    // counts the visit; the 1/t stage keeps them in lane 0's branch
-                    if constexpr (!kIT) {
-                        lg_s[cur - wb] = lg_cur;
-                        act_s[ncur - wb] = 1;
-                        if (lane == 0) atomicAdd(&hd[ncur - wb], 1u);
-                    } else if (lane == 0) {
-                        lg_s[cur - wb] = lg_cur;
-                        atomicAdd(&hd[ncur - wb], 1u);
-                        act_s[ncur - wb] = 1;
-                    }
+                    hcnt = (move ? hd_load : hcnt) + 1u;
+                    // every lane stores the same values (no branch, no atomic, no warp barrier:
+                    // each lane reads back only what it has stored itself)
+                    lg_s[cur - wb] = lg_cur;
+                    hd[ncur - wb] = hcnt;
+                    act_s[ncur - wb] = 1;
+                    cur_vis = true;
                     cur = ncur;
                     if (kIT) {
                         lg_base_p = lg_base;
@@ -357,9 +379,6 @@ __global__ void __launch_bounds__(64 * kWindowMaxWalkers, 1) sweep_window_kernel
                     } else {
                         lg_cur = frozen ? lg_base : lg_base + factor;
                     }
-                    __syncwarp();  // the stores are visible to every lane
-                    // draws before this site are done (in the Wang-Landau stage every lane stores the value)
-                    if (!kIT || lane == 0) st_release_u32(consumed_addr, hq);
                     hq += need_u ? 2u : 1u;
                     i = c;
                     h = h_next;

@@ -173,6 +173,20 @@ __device__ __forceinline__ double inverse_time_factor_select(InverseTimeTable32&
     const double q = __shfl_sync(kFull, T.q, static_cast<int>(T.next++));
     return active_bins == 0 ? current : q;
 }
+// The same table with the refresh taken out of the per-attempt path: a caller that tests
+// (T.next >= 32 || active_bins != T.active) in a branch of its own calls the refresh there,
+// before the attempt, with the attempts made so far; the factor of the attempt is then a
+// shuffle and a select.
+__device__ __forceinline__ void inverse_time_refresh(InverseTimeTable32& T, uint64_t attempted_before,
+                                                     uint32_t active_bins, int lane) {
+    T.active = active_bins;
+    T.next = 0;
+    T.q = static_cast<double>(active_bins) / static_cast<double>(attempted_before + static_cast<uint64_t>(lane) + 1);
+}
+__device__ __forceinline__ double inverse_time_factor_next(InverseTimeTable32& T, uint32_t active_bins, double current) {
+    const double q = __shfl_sync(kFull, T.q, static_cast<int>(T.next++));
+    return active_bins == 0 ? current : q;
+}
 
 // Floor of a bin coordinate 0 <= q < 2^31 (the grid index of an in-range energy): the sum
 // q + 2^52 rounded toward -infinity is 2^52 + floor(q) exactly (the unit in the last place is
