@@ -22,7 +22,7 @@
 // * The producer generates the walker's draws 32 at a time (every lane steps the generator,
 //   lane j keeps draw j, with its site and log(max(u, 2^-53)), src/wang_landau.cpp:250, 261)
 //   into a 64-entry shared-memory ring, published with release stores; the walker publishes
-//   the draws it has consumed.  The draw stream runs on across the epochs of the launch; at
+//   the draws it has consumed once per batch of 32.  The draw stream runs on across the epochs of the launch; at
 //   the end the generator is stepped back over the draws not consumed (rng_step_back).
 // * At the end of an epoch each walker folds its histogram deltas, runs the check, and the
 //   walker warps meet at a named barrier (the producers never take part); walker 0 decides
